@@ -1,0 +1,292 @@
+"""Python host mirror of the csmg / libcsm interface (ctypes over include/csm.h).
+
+The reference (gh8li/GCSM-BU) is driven by its `csmg` process: main.cpp:162-190 parses the
+flags, technique_permutation.h:29-225 loads the query, the data graph and the update stream and
+runs the per-batch loop.  `Engine` exposes the same steps as methods over libcsm.so, and
+`run_csmg_like` replays a whole stream the way the reference's driver does.
+
+The CUDA library is the only compute path: importing this module on a machine without the
+built library, or calling it without a B200, raises instead of falling back to anything else.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_HERE), "lib", "libcsm.so")
+CSMG_PATH = os.path.join(os.path.dirname(_HERE), "bin", "csmg")
+
+CSM_OK = 0
+ERRORS = {
+    -1: "invalid argument",
+    -2: "CUDA error",
+    -3: "out of memory",
+    -4: "timeout",
+    -5: "bad state",
+    -6: "limit exceeded",
+    -7: "overflow",
+    -8: "no device",
+}
+
+# Every symbol declared in include/csm.h.
+EXPORTED = [
+    "csm_default_config", "csm_create", "csm_destroy", "csm_load_query", "csm_load_graph",
+    "csm_apply_batch", "csm_apply_batch_device", "csm_get_edge_counts", "csm_get_embeddings",
+    "csm_free", "csm_describe_plan", "csm_get_stats", "csm_reset_stats", "csm_device_memory",
+    "csm_last_error", "csm_version",
+]
+
+
+class CsmConfig(ctypes.Structure):
+    _fields_ = [
+        ("device", ctypes.c_int32),
+        ("algorithm", ctypes.c_int32),
+        ("matching_order", ctypes.c_int32),
+        ("search_strategy", ctypes.c_int32),
+        ("local_index", ctypes.c_int32),
+        ("cartesian_product", ctypes.c_int32),
+        ("heavy_vertex_avoidance", ctypes.c_int32),
+        ("relation_switch", ctypes.c_int32),
+        ("pool_entries", ctypes.c_uint64),
+        ("max_batch", ctypes.c_uint64),
+        ("frontier_bytes", ctypes.c_uint64),
+        ("materialize_rows", ctypes.c_uint64),
+        ("blocks_per_sm", ctypes.c_int32),
+        ("warps_per_block", ctypes.c_int32),
+        ("steal_chunk", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 5),
+    ]
+
+
+class CsmBatchResult(ctypes.Structure):
+    _fields_ = [
+        ("positive", ctypes.c_uint64),
+        ("negative", ctypes.c_uint64),
+        ("inserted", ctypes.c_uint64),
+        ("deleted", ctypes.c_uint64),
+        ("latency_ns", ctypes.c_uint64),
+        ("apply_ns", ctypes.c_uint64),
+        ("enum_ns", ctypes.c_uint64),
+        ("reserved", ctypes.c_uint64),
+    ]
+
+
+class CsmStats(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_uint64) for name in (
+        "batches", "enum_launches", "kernel_launches", "enum_scan_entries", "enum_probes",
+        "enum_tail_lists", "donations", "enum_ns", "apply_ns", "pool_used", "pool_capacity",
+        "compactions")] + [("reserved", ctypes.c_uint64 * 4)]
+
+
+class CsmError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"csm error {code} ({ERRORS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Loads libcsm.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is missing: build it with `make -C gcsm-bu_b200`")
+    lib = ctypes.CDLL(path)
+    u32p = ctypes.POINTER(ctypes.c_uint32)
+    u8p = ctypes.POINTER(ctypes.c_uint8)
+    u64p = ctypes.POINTER(ctypes.c_uint64)
+    vp = ctypes.c_void_p
+    lib.csm_version.restype = ctypes.c_char_p
+    lib.csm_default_config.argtypes = [ctypes.POINTER(CsmConfig)]
+    lib.csm_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(CsmConfig)]
+    lib.csm_destroy.argtypes = [vp]
+    lib.csm_load_query.argtypes = [vp, ctypes.c_uint32, u32p, ctypes.c_uint32, u32p, u32p, u32p,
+                                   ctypes.POINTER(ctypes.c_int32)]
+    lib.csm_load_graph.argtypes = [vp, ctypes.c_uint32, u32p, ctypes.c_uint64, u32p, u32p, u32p]
+    lib.csm_apply_batch.argtypes = [vp, ctypes.c_uint64, u32p, u32p, u32p, u8p, ctypes.POINTER(CsmBatchResult)]
+    lib.csm_apply_batch_device.argtypes = [vp, ctypes.c_uint64, vp, vp, vp, vp, vp, ctypes.POINTER(CsmBatchResult)]
+    lib.csm_get_edge_counts.argtypes = [vp, ctypes.c_int32, u64p, u64p, ctypes.c_uint32, u32p]
+    lib.csm_get_embeddings.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(u32p), u64p]
+    lib.csm_free.argtypes = [vp]
+    lib.csm_describe_plan.argtypes = [vp, ctypes.c_int32, ctypes.c_char_p, ctypes.c_size_t]
+    lib.csm_get_stats.argtypes = [vp, ctypes.POINTER(CsmStats)]
+    lib.csm_reset_stats.argtypes = [vp]
+    lib.csm_device_memory.argtypes = [vp, u64p, u64p]
+    lib.csm_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
+    for name in EXPORTED:
+        if name != "csm_version":
+            getattr(lib, name).restype = ctypes.c_int32
+    _lib = lib
+    return lib
+
+
+def _u32(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.uint32))
+
+
+def _ptr(a: np.ndarray, ctype=ctypes.c_uint32):
+    return a.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+def default_config(**overrides) -> CsmConfig:
+    lib = load_library()
+    cfg = CsmConfig()
+    lib.csm_default_config(ctypes.byref(cfg))
+    for k, v in overrides.items():
+        setattr(cfg, k, v)
+    return cfg
+
+
+@dataclass
+class QueryGraph:
+    """A labelled query: vertices 0..nv-1 with labels, undirected labelled edges."""
+    vlabels: np.ndarray
+    src: np.ndarray
+    dst: np.ndarray
+    elabels: np.ndarray
+
+    @property
+    def nv(self) -> int:
+        return int(len(self.vlabels))
+
+
+@dataclass
+class DataGraph:
+    vlabels: np.ndarray
+    src: np.ndarray
+    dst: np.ndarray
+    elabels: np.ndarray
+
+
+@dataclass
+class Batch:
+    src: np.ndarray
+    dst: np.ndarray
+    elabels: np.ndarray
+    is_delete: Optional[np.ndarray] = None
+
+
+class Engine:
+    """One libcsm engine on one GPU (csm_create .. csm_destroy)."""
+
+    def __init__(self, config: Optional[CsmConfig] = None, **overrides):
+        self.lib = load_library()
+        cfg = config if config is not None else default_config()
+        for k, v in overrides.items():
+            setattr(cfg, k, v)
+        self.config = cfg
+        self._h = ctypes.c_void_p()
+        rc = self.lib.csm_create(ctypes.byref(self._h), ctypes.byref(cfg))
+        if rc != CSM_OK:
+            raise CsmError(rc, self._err(None))
+        self.queries: List[QueryGraph] = []
+
+    def _err(self, h) -> str:
+        buf = ctypes.create_string_buffer(1024)
+        self.lib.csm_last_error(h, buf, len(buf))
+        return buf.value.decode(errors="replace")
+
+    def _check(self, rc: int):
+        if rc != CSM_OK:
+            raise CsmError(rc, self._err(self._h))
+
+    def close(self):
+        if self._h:
+            self.lib.csm_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def load_query(self, q: QueryGraph) -> int:
+        vl, s, d, l = _u32(q.vlabels), _u32(q.src), _u32(q.dst), _u32(q.elabels)
+        qid = ctypes.c_int32(-1)
+        self._check(self.lib.csm_load_query(self._h, len(vl), _ptr(vl), len(s), _ptr(s), _ptr(d), _ptr(l),
+                                            ctypes.byref(qid)))
+        self.queries.append(q)
+        return qid.value
+
+    def load_graph(self, g: DataGraph):
+        vl, s, d, l = _u32(g.vlabels), _u32(g.src), _u32(g.dst), _u32(g.elabels)
+        self._check(self.lib.csm_load_graph(self._h, len(vl), _ptr(vl), len(s), _ptr(s), _ptr(d), _ptr(l)))
+
+    def apply(self, b: Batch) -> List[CsmBatchResult]:
+        s, d, l = _u32(b.src), _u32(b.dst), _u32(b.elabels)
+        out = (CsmBatchResult * max(1, len(self.queries)))()
+        dp = None
+        if b.is_delete is not None:
+            dl = np.ascontiguousarray(np.asarray(b.is_delete, dtype=np.uint8))
+            dp = _ptr(dl, ctypes.c_uint8)
+        self._check(self.lib.csm_apply_batch(self._h, len(s), _ptr(s), _ptr(d), _ptr(l), dp, out))
+        return list(out)[: len(self.queries)]
+
+    def apply_device(self, n: int, src_ptr: int, dst_ptr: int, lab_ptr: int, del_ptr: Optional[int] = None,
+                     stream: Optional[int] = None) -> List[CsmBatchResult]:
+        out = (CsmBatchResult * max(1, len(self.queries)))()
+        self._check(self.lib.csm_apply_batch_device(self._h, n, ctypes.c_void_p(src_ptr), ctypes.c_void_p(dst_ptr),
+                                                    ctypes.c_void_p(lab_ptr),
+                                                    ctypes.c_void_p(del_ptr) if del_ptr else None,
+                                                    ctypes.c_void_p(stream) if stream else None, out))
+        return list(out)[: len(self.queries)]
+
+    def edge_counts(self, qid: int):
+        n = ctypes.c_uint32()
+        pos = (ctypes.c_uint64 * 64)()
+        neg = (ctypes.c_uint64 * 64)()
+        self._check(self.lib.csm_get_edge_counts(self._h, qid, pos, neg, 64, ctypes.byref(n)))
+        return list(pos)[: n.value], list(neg)[: n.value]
+
+    def embeddings(self, qid: int, sign: int = 1) -> np.ndarray:
+        rows = ctypes.POINTER(ctypes.c_uint32)()
+        nrows = ctypes.c_uint64()
+        self._check(self.lib.csm_get_embeddings(self._h, qid, sign, ctypes.byref(rows), ctypes.byref(nrows)))
+        nv = self.queries[qid].nv
+        try:
+            if nrows.value == 0:
+                return np.zeros((0, nv), dtype=np.uint32)
+            arr = np.ctypeslib.as_array(rows, shape=(nrows.value * nv,)).copy()
+        finally:
+            self.lib.csm_free(rows)
+        return arr.reshape(-1, nv)
+
+    def describe(self, qid: int) -> str:
+        buf = ctypes.create_string_buffer(1 << 16)
+        self._check(self.lib.csm_describe_plan(self._h, qid, buf, len(buf)))
+        return buf.value.decode()
+
+    def stats(self) -> CsmStats:
+        st = CsmStats()
+        self._check(self.lib.csm_get_stats(self._h, ctypes.byref(st)))
+        return st
+
+    def reset_stats(self):
+        self._check(self.lib.csm_reset_stats(self._h))
+
+
+def version() -> str:
+    return load_library().csm_version().decode()
+
+
+def run_csmg_like(query: QueryGraph, data: DataGraph, batches: Sequence[Batch], **config) -> List[List[CsmBatchResult]]:
+    """Replays a stream the way technique_permutation.h:29-225 does: load, then one call per batch."""
+    with Engine(**config) as eng:
+        eng.load_query(query)
+        eng.load_graph(data)
+        return [eng.apply(b) for b in batches]

@@ -1,0 +1,121 @@
+// Shared host/device definitions of the B200 continuous subgraph matching engine.
+//
+// Device graph layout (replaces CSR_GPU / RelationsGPU of graph/match_gpu.h:20-47):
+//  - A *relation* is a directed label triple (src vertex label, edge label, dst vertex label)
+//    that occurs as the orientation of some query edge.  The reference keeps one relation per
+//    directed query edge (edge_idx, graph/graph.cpp:438-459); here query edges with the same
+//    triple share one relation, and the per-query-edge differences (which updated edges an
+//    edge may use) are expressed by a flag on each adjacency entry instead of by copies.
+//  - meta[rel * V + v] = {offset, size} of v's sorted adjacency list inside `pool`;
+//    cap[rel * V + v] = its slack capacity (power of two, at least 8, as indexing.cu:46-59).
+//  - An adjacency entry is (neighbour << 1) | flag.  flag = 1 marks an edge that is part of
+//    the batch being processed (inserted in the insertion phase, about to be deleted in the
+//    deletion phase).  Sorting by entry sorts by neighbour id.
+#pragma once
+
+#include <stdint.h>
+
+#define CSM_MAXQV 16
+#define CSM_MAXQE 42
+#define CSM_MAXBN 15
+#define CSM_WARP 32
+#define CSM_NO_REL 0xFFFFu
+#define CSM_NO_LABEL 0xFFu
+#define CSM_INVALID_KEY 0xFFFFFFFFFFFFFFFFull
+
+// Effect of one sorted batch key after classification.
+#define CSM_EFF_NONE 0
+#define CSM_EFF_INS 1
+#define CSM_EFF_DEL 2
+
+// Phase of an enumeration launch; equals the CSM_EFF_* value its seeds carry.
+#define CSM_PHASE_INS 1
+#define CSM_PHASE_DEL 2
+
+// Maximum tail-leaf bookkeeping of one plan (Cartesian flattening, kernels/cartesian_product.cu).
+#define CSM_TAIL_MAXKEYS 8
+#define CSM_TAIL_MAXMASKS 32
+#define CSM_TAIL_MAXCLASSES 8
+
+// One matching-order level (one query vertex) of a plan.
+struct DevLevel {
+    uint16_t bn_rel[CSM_MAXBN];   // relation of (backward neighbour -> this vertex)
+    uint8_t bn_depth[CSM_MAXBN];  // depth of each backward neighbour in the order
+    uint8_t nbn;                  // number of backward neighbours
+    uint16_t old_mask;            // bit k: backward edge k must not be a batch edge
+    uint8_t qv;                   // query vertex id
+    uint8_t pad0;
+    uint32_t nlf_bitmap;          // candidate bitmap (NLF filter) of this query vertex
+    uint32_t pad1[2];
+};
+
+struct DevTailTerm {
+    int64_t coef;
+    uint8_t nf;                    // number of factors
+    uint8_t f[7];                  // mask ids
+};
+
+// Cartesian tail of a plan: query vertices at depth >= tail_start are leaves whose only
+// neighbour is matched earlier (plan.cpp:1785-1841 TreeCartesianProduct).  Their number of
+// injective assignments is counted by inclusion-exclusion over the leaves of one label.
+struct DevTail {
+    uint8_t nkeys;                              // distinct (parent depth, relation, old) lists
+    uint8_t key_parent[CSM_TAIL_MAXKEYS];
+    uint8_t key_old[CSM_TAIL_MAXKEYS];
+    uint16_t key_rel[CSM_TAIL_MAXKEYS];
+    uint8_t nmasks;                             // key subsets whose intersection size is used
+    uint8_t nclasses;
+    uint16_t mask[CSM_TAIL_MAXMASKS];
+    uint16_t class_term_begin[CSM_TAIL_MAXCLASSES + 1];  // into the plan's term list
+};
+
+// One (query, updated query edge) pair: the unit of the per-batch decomposition of
+// technique_permutation.h:125-212.
+struct DevPlan {
+    uint16_t query;
+    uint8_t n;             // number of query vertices
+    uint8_t qe;            // index of the updated query edge in qe_list_
+    uint8_t tail_start;    // first depth of the Cartesian tail (== n when there is none)
+    uint8_t materialize;   // 1: write full rows instead of counting the tail
+    uint16_t seed_rel;     // relation of (order[0] -> order[1])
+    uint8_t order[CSM_MAXQV];
+    uint32_t nlf0, nlf1;   // candidate bitmaps of order[0] and order[1]
+    uint32_t term_begin;   // tail polynomial terms in the global term array
+    uint32_t nterms;
+    DevLevel lv[CSM_MAXQV];
+    DevTail tail;
+};
+
+// Work item of the persistent enumeration: a partial embedding with `depth` fixed vertices
+// and the range [lo, hi) of candidates still to scan at level `depth` (for depth 0 the range
+// indexes seed positions in the sorted batch).
+struct WorkItem {
+    uint32_t plan;
+    uint32_t depth;
+    uint32_t lo;
+    uint32_t hi;
+    uint32_t f[CSM_MAXQV];
+};
+
+// Device-side control block of one enumeration launch.
+struct EnumControl {
+    unsigned long long ticket;        // next seed / frontier ticket
+    unsigned long long nticket;       // total tickets
+    unsigned int q_write;             // donation slots reserved
+    unsigned int q_read;              // donation slots claimed
+    unsigned int hungry;              // warps waiting for work
+    unsigned int active;              // warps holding work
+    unsigned int error;               // bit 0 timeout, bit 1 output overflow, bit 2 queue overflow
+    unsigned int epoch;               // launch epoch, marks ready slots
+    unsigned long long out_rows;      // rows written (materialize / expand)
+    unsigned long long scan_entries;  // statistics
+    unsigned long long probes;
+    unsigned long long tail_lists;
+    unsigned long long donations;
+    unsigned long long expand_bound;  // upper bound of the next BFS level
+};
+
+#define CSM_ERRBIT_TIMEOUT 1u
+#define CSM_ERRBIT_OUTPUT 2u
+#define CSM_ERRBIT_QUEUE 4u
+#define CSM_ERRBIT_POOL 8u

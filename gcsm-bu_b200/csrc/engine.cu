@@ -1,0 +1,761 @@
+// Engine orchestration: set-up, initial load, the per-batch pipeline and result readback.
+#include "engine.h"
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <sstream>
+
+namespace csm {
+
+namespace {
+
+uint32_t bits_for(uint64_t v) {  // bits needed to represent 0..v
+    uint32_t b = 1;
+    while (b < 64 && (v >> b) != 0) b++;
+    return b;
+}
+
+template <typename T>
+cudaError_t dalloc(T **p, size_t count) {
+    return cudaMalloc((void **)p, sizeof(T) * (count ? count : 1));
+}
+
+}  // namespace
+
+Options resolve_options(const csm_config &cfg) {
+    Options o;
+    switch (cfg.algorithm) {
+        case 1:  // GCSM-BU
+            o = {Order::kGcsm, 2, true, true, true, true};
+            break;
+        case 2:  // QO-GAMMA
+            o = {Order::kGamma, 0, false, true, false, false};
+            break;
+        case 4:
+            o = {Order::kIndexing, 2, false, true, true, true};
+            break;
+        case 5:
+            o = {Order::kGamma, 2, false, true, true, true};
+            break;
+        default: {
+            o.order = cfg.matching_order >= 0 && cfg.matching_order <= 3 ? (Order)cfg.matching_order : Order::kGcsm;
+            o.search_strategy = cfg.search_strategy >= 0 && cfg.search_strategy <= 3 ? cfg.search_strategy : 2;
+            o.local_index = cfg.local_index != 0;
+            o.cartesian = cfg.cartesian_product != 0;
+            o.heavy_vertex_avoidance = cfg.heavy_vertex_avoidance != 0;
+            o.relation_switch = cfg.relation_switch != 0;
+        }
+    }
+    return o;
+}
+
+Engine::Engine(const csm_config &cfg) : cfg_(cfg), opt_(resolve_options(cfg)) {}
+
+csm_status Engine::fail(csm_status code, const std::string &msg) {
+    err_ = msg;
+    return code;
+}
+
+csm_status Engine::cuda_fail(cudaError_t e, const char *where) {
+    err_ = std::string(where) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? CSM_ERR_OOM : CSM_ERR_CUDA;
+}
+
+#define CSM_CUDA(call)                                   \
+    do {                                                 \
+        cudaError_t e__ = (call);                        \
+        if (e__ != cudaSuccess) return cuda_fail(e__, #call); \
+    } while (0)
+
+csm_status Engine::init() {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(CSM_ERR_NO_DEVICE, "no CUDA device");
+    if (cfg_.device < 0 || cfg_.device >= ndev) return fail(CSM_ERR_INVALID_ARG, "device ordinal out of range");
+    device_ = cfg_.device;
+    CSM_CUDA(cudaSetDevice(device_));
+    cudaDeviceProp prop;
+    CSM_CUDA(cudaGetDeviceProperties(&prop, device_));
+    if (prop.major < 10) return fail(CSM_ERR_NO_DEVICE, "this library is built for sm_100a (B200)");
+    sm_count_ = prop.multiProcessorCount;
+    CSM_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    for (auto &e : ev_) CSM_CUDA(cudaEventCreate(&e));
+    warps_per_block_ = cfg_.warps_per_block > 0 && cfg_.warps_per_block <= 8 ? cfg_.warps_per_block : 8;
+    const int bps = cfg_.blocks_per_sm > 0 ? cfg_.blocks_per_sm : 4;
+    blocks_ = sm_count_ * bps;
+    CSM_CUDA(dalloc(&d_ctrl_, 1));
+    CSM_CUDA(dalloc(&d_misc_, 8));
+    CSM_CUDA(cudaMallocHost(&h_counts_, sizeof(unsigned long long) * 64));
+    CSM_CUDA(cudaMallocHost(&h_ctrl_, sizeof(EnumControl) * 2));
+    return CSM_OK;
+}
+
+Engine::~Engine() {
+    if (stream_) cudaStreamSynchronize(stream_);
+    void *dev[] = {d_elab_raw_, d_rel_table_, d_spec_begin_, d_specs_, d_bits_, g_.meta, g_.cap, g_.pool, g_.pool_top,
+                   g_.vlab, d_plans_, d_terms_, d_upd_src_, d_upd_dst_, d_upd_lab_, d_upd_del_, d_keys_raw_, d_keys_,
+                   d_sort_temp_, bs_.eff, bs_.heads, bs_.nheads, bs_.seg_nins, bs_.seg_ndel, bs_.seg_end, bs_.scr_y,
+                   bs_.scr_lb, bs_.counters, bs_.error, d_ctrl_, d_queue_, d_ready_, d_seed_lo_, d_ticket_prefix_,
+                   d_counts_, d_frontier_[0], d_frontier_[1], d_rows_, d_misc_};
+    for (void *p : dev)
+        if (p) cudaFree(p);
+    if (h_pin_) cudaFreeHost(h_pin_);
+    if (h_counts_) cudaFreeHost(h_counts_);
+    if (h_ctrl_) cudaFreeHost(h_ctrl_);
+    for (auto &e : ev_)
+        if (e) cudaEventDestroy(e);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+csm_status Engine::load_query(uint32_t nv, const uint32_t *vlabel, uint32_t ne, const uint32_t *src,
+                              const uint32_t *dst, const uint32_t *elabel, int32_t *qid) {
+    if (graph_loaded_) return fail(CSM_ERR_STATE, "queries must be registered before the data graph is loaded");
+    if (!vlabel || !src || !dst || !elabel) return fail(CSM_ERR_INVALID_ARG, "null query array");
+    Query q;
+    std::string why = build_query(nv, vlabel, ne, src, dst, elabel, q);
+    if (!why.empty()) return fail(CSM_ERR_LIMIT, why);
+    if (queries_.size() >= 4096) return fail(CSM_ERR_LIMIT, "too many standing queries");
+    queries_.push_back(std::move(q));
+    if (qid) *qid = (int32_t)queries_.size() - 1;
+    return CSM_OK;
+}
+
+csm_status Engine::load_graph(uint32_t nv, const uint32_t *vlabel, uint64_t ne, const uint32_t *src,
+                              const uint32_t *dst, const uint32_t *elabel) {
+    if (graph_loaded_) return fail(CSM_ERR_STATE, "the data graph is already loaded");
+    if (queries_.empty()) return fail(CSM_ERR_STATE, "register at least one query before loading the graph");
+    if (nv == 0 || !vlabel) return fail(CSM_ERR_INVALID_ARG, "empty vertex set");
+    if (ne && (!src || !dst || !elabel)) return fail(CSM_ERR_INVALID_ARG, "null edge array");
+    CSM_CUDA(cudaSetDevice(device_));
+    // Label spaces: the union of the labels of all queries (graph.cpp:389-433 keeps only
+    // data labels that occur in the query).
+    for (auto &q : queries_) {
+        vlab_raw_.insert(vlab_raw_.end(), q.vlabel.begin(), q.vlabel.end());
+        elab_raw_.insert(elab_raw_.end(), q.qe_elabel.begin(), q.qe_elabel.end());
+    }
+    std::sort(vlab_raw_.begin(), vlab_raw_.end());
+    vlab_raw_.erase(std::unique(vlab_raw_.begin(), vlab_raw_.end()), vlab_raw_.end());
+    std::sort(elab_raw_.begin(), elab_raw_.end());
+    elab_raw_.erase(std::unique(elab_raw_.begin(), elab_raw_.end()), elab_raw_.end());
+    if (vlab_raw_.size() >= CSM_NO_LABEL || elab_raw_.size() >= 255)
+        return fail(CSM_ERR_LIMIT, "too many distinct labels across the registered queries");
+    const uint32_t nvl = (uint32_t)vlab_raw_.size(), nel = (uint32_t)elab_raw_.size();
+    auto vl = [&](uint32_t raw) {
+        return (uint32_t)(std::lower_bound(vlab_raw_.begin(), vlab_raw_.end(), raw) - vlab_raw_.begin());
+    };
+    auto el = [&](uint32_t raw) {
+        return (uint32_t)(std::lower_bound(elab_raw_.begin(), elab_raw_.end(), raw) - elab_raw_.begin());
+    };
+    // Relations: one per directed label triple of any query edge.
+    rel_table_.assign((size_t)nvl * nel * nvl, CSM_NO_REL);
+    auto rel_of_raw = [&](uint32_t a_raw, uint32_t l_raw, uint32_t b_raw) -> uint16_t {
+        const size_t idx = ((size_t)vl(a_raw) * nel + el(l_raw)) * nvl + vl(b_raw);
+        if (rel_table_[idx] == CSM_NO_REL) {
+            rel_table_[idx] = (uint16_t)rel_triples_.size();
+            rel_triples_.push_back((vl(a_raw) << 16) | (el(l_raw) << 8) | vl(b_raw));
+        }
+        return rel_table_[idx];
+    };
+    for (auto &q : queries_)
+        for (uint32_t u = 0; u < q.nv; u++)
+            for (auto &p : q.nbrs[u]) rel_of_raw(q.vlabel[u], p.second, q.vlabel[p.first]);
+    if (rel_triples_.size() >= CSM_NO_REL) return fail(CSM_ERR_LIMIT, "too many relations");
+    // NLF specs per dense label.
+    std::vector<std::vector<NlfSpec>> by_label(nvl);
+    nbitmaps_ = 0;
+    for (auto &q : queries_) {
+        nlf_base_.push_back(nbitmaps_);
+        for (uint32_t u = 0; u < q.nv; u++) {
+            NlfSpec sp{};
+            sp.bitmap = nbitmaps_ + u;
+            sp.ngroups = (uint32_t)q.nlf[u].size();
+            for (uint32_t g = 0; g < sp.ngroups; g++) {
+                sp.rel[g] = rel_of_raw(q.vlabel[u], q.nlf[u][g].elabel, q.nlf[u][g].vlabel);
+                sp.cnt[g] = (uint16_t)q.nlf[u][g].count;
+            }
+            by_label[vl(q.vlabel[u])].push_back(sp);
+        }
+        nbitmaps_ += q.nv;
+    }
+    std::vector<uint32_t> spec_begin(nvl + 1, 0);
+    std::vector<NlfSpec> specs;
+    for (uint32_t a = 0; a < nvl; a++) {
+        spec_begin[a] = (uint32_t)specs.size();
+        specs.insert(specs.end(), by_label[a].begin(), by_label[a].end());
+    }
+    spec_begin[nvl] = (uint32_t)specs.size();
+
+    g_.V = nv;
+    g_.R = (uint32_t)rel_triples_.size();
+    kl_.vbits = bits_for(nv ? nv - 1 : 0);
+    kl_.rbits = bits_for(g_.R);
+    if (kl_.end_bit() > 64) return fail(CSM_ERR_LIMIT, "vertex ids and relations do not fit a 64-bit batch key");
+    words_ = (nv + 31) / 32;
+
+    // Dense vertex labels.
+    std::vector<uint8_t> vlab(nv, CSM_NO_LABEL);
+    for (uint32_t v = 0; v < nv; v++) {
+        auto it = std::lower_bound(vlab_raw_.begin(), vlab_raw_.end(), vlabel[v]);
+        if (it != vlab_raw_.end() && *it == vlabel[v]) vlab[v] = (uint8_t)(it - vlab_raw_.begin());
+    }
+    const size_t nmeta = (size_t)g_.R * nv;
+    CSM_CUDA(dalloc(&g_.vlab, nv));
+    CSM_CUDA(cudaMemcpy(g_.vlab, vlab.data(), nv, cudaMemcpyHostToDevice));
+    CSM_CUDA(dalloc(&d_elab_raw_, nel));
+    CSM_CUDA(cudaMemcpy(d_elab_raw_, elab_raw_.data(), sizeof(uint32_t) * nel, cudaMemcpyHostToDevice));
+    CSM_CUDA(dalloc(&d_rel_table_, rel_table_.size()));
+    CSM_CUDA(cudaMemcpy(d_rel_table_, rel_table_.data(), sizeof(uint16_t) * rel_table_.size(), cudaMemcpyHostToDevice));
+    CSM_CUDA(dalloc(&d_spec_begin_, nvl + 1));
+    CSM_CUDA(cudaMemcpy(d_spec_begin_, spec_begin.data(), sizeof(uint32_t) * (nvl + 1), cudaMemcpyHostToDevice));
+    CSM_CUDA(dalloc(&d_specs_, specs.size()));
+    if (!specs.empty())
+        CSM_CUDA(cudaMemcpy(d_specs_, specs.data(), sizeof(NlfSpec) * specs.size(), cudaMemcpyHostToDevice));
+    CSM_CUDA(dalloc(&d_bits_, (size_t)nbitmaps_ * words_));
+    CSM_CUDA(cudaMemset(d_bits_, 0, sizeof(uint32_t) * (size_t)nbitmaps_ * words_));
+    CSM_CUDA(dalloc(&g_.meta, nmeta));
+    CSM_CUDA(dalloc(&g_.cap, nmeta));
+    CSM_CUDA(dalloc(&g_.pool_top, 1));
+
+    // Edges -> keys -> sorted -> lists.
+    const uint64_t m64 = 2 * ne;
+    if (m64 >= 0x7FFFFFFFull) return fail(CSM_ERR_LIMIT, "too many initial edges for one load (limit 2^30)");
+    const uint32_t m = (uint32_t)m64;
+    uint32_t *d_src = nullptr, *d_dst = nullptr, *d_lab = nullptr;
+    unsigned long long *k_raw = nullptr, *k_sorted = nullptr;
+    void *temp = nullptr;
+    size_t temp_bytes = 0;
+    LabelTables lt{d_elab_raw_, nel, d_rel_table_, nvl};
+    csm_status st = CSM_OK;
+    std::string berr;
+    do {
+        cudaError_t e;
+        if ((e = dalloc(&d_src, ne)) || (e = dalloc(&d_dst, ne)) || (e = dalloc(&d_lab, ne)) ||
+            (e = dalloc(&k_raw, m)) || (e = dalloc(&k_sorted, m))) {
+            st = cuda_fail(e, "initial edge buffers");
+            break;
+        }
+        if (ne) {
+            cudaMemcpy(d_src, src, sizeof(uint32_t) * ne, cudaMemcpyHostToDevice);
+            cudaMemcpy(d_dst, dst, sizeof(uint32_t) * ne, cudaMemcpyHostToDevice);
+            cudaMemcpy(d_lab, elabel, sizeof(uint32_t) * ne, cudaMemcpyHostToDevice);
+            store_build_keys(ne, d_src, d_dst, d_lab, nullptr, lt, g_, kl_, k_raw, stream_);
+        }
+        store_sort_keys(nullptr, temp_bytes, k_raw, k_sorted, m, kl_, stream_);
+        if ((e = cudaMalloc(&temp, temp_bytes + 16))) {
+            st = cuda_fail(e, "sort scratch");
+            break;
+        }
+        if (m) store_sort_keys(temp, temp_bytes, k_raw, k_sorted, m, kl_, stream_);
+        cudaFree(d_src);
+        cudaFree(d_dst);
+        cudaFree(d_lab);
+        d_src = d_dst = d_lab = nullptr;
+        cudaFree(k_raw);
+        k_raw = nullptr;
+        // Pool: the laid-out lists plus room for batches; compaction regrows it later.
+        const uint64_t max_batch = cfg_.max_batch ? cfg_.max_batch : (1ull << 20);
+        unsigned long long want = cfg_.pool_entries ? cfg_.pool_entries
+                                                    : (unsigned long long)(10 * m64 + 64 * max_batch + (1u << 20));
+        if (want > 0xFFFFFFF0ull) want = 0xFFFFFFF0ull;
+        g_.pool_cap = want;
+        if ((e = dalloc(&g_.pool, g_.pool_cap))) {
+            st = cuda_fail(e, "adjacency pool");
+            break;
+        }
+        if ((e = store_build_from_keys(g_, k_sorted, m, kl_, stream_, berr))) {
+            st = berr.empty() ? cuda_fail(e, "initial build") : fail(CSM_ERR_OOM, berr);
+            break;
+        }
+    } while (false);
+    cudaFree(d_src);
+    cudaFree(d_dst);
+    cudaFree(d_lab);
+    cudaFree(k_raw);
+    cudaFree(k_sorted);
+    cudaFree(temp);
+    if (st != CSM_OK) return st;
+
+    // Candidate bitmaps, planner statistics, plans.
+    NlfTables nt{d_spec_begin_, d_specs_, d_bits_, words_};
+    store_nlf_all(g_, nt, stream_);
+    unsigned long long *d_stat = nullptr;
+    CSM_CUDA(dalloc(&d_stat, 2));
+    std::vector<EdgeStats> stats(queries_.size());
+    for (size_t qi = 0; qi < queries_.size(); qi++) {
+        const Query &q = queries_[qi];
+        stats[qi].card.assign(q.nv * q.nv, 0);
+        stats[qi].avg.assign(q.nv * q.nv, 0.f);
+        for (uint32_t u = 0; u < q.nv; u++)
+            for (auto &p : q.nbrs[u]) {
+                const uint32_t uu = p.first;
+                const uint16_t rel = rel_table_[((size_t)vl(q.vlabel[u]) * nel + el(p.second)) * nvl + vl(q.vlabel[uu])];
+                CSM_CUDA(cudaMemsetAsync(d_stat, 0, 16, stream_));
+                store_edge_stats(g_, rel, d_bits_ + (size_t)(nlf_base_[qi] + u) * words_,
+                                 d_bits_ + (size_t)(nlf_base_[qi] + uu) * words_, d_stat, stream_);
+                unsigned long long h[2];
+                CSM_CUDA(cudaMemcpyAsync(h, d_stat, 16, cudaMemcpyDeviceToHost, stream_));
+                CSM_CUDA(cudaStreamSynchronize(stream_));
+                stats[qi].card[u * q.nv + uu] = (uint32_t)std::min<unsigned long long>(h[0], 0xFFFFFFFFull);
+                // GetSummary divides by the number of sources (match_gpu.cu:607), NaN when empty.
+                stats[qi].avg[u * q.nv + uu] = (float)h[0] / (float)h[1];
+            }
+    }
+    cudaFree(d_stat);
+    for (size_t qi = 0; qi < queries_.size(); qi++) {
+        const Query &q = queries_[qi];
+        PlanOptions po;
+        po.order = opt_.order;
+        po.cartesian = opt_.cartesian;
+        po.materialize = cfg_.materialize_rows > 0;
+        auto rel_of = [&](uint32_t u, uint32_t uu) -> uint16_t {
+            return rel_table_[((size_t)vl(q.vlabel[u]) * nel + el(q.edge_label(u, uu))) * nvl + vl(q.vlabel[uu])];
+        };
+        auto ps = build_plans(q, (uint16_t)qi, nlf_base_[qi], stats[qi], po, rel_of);
+        plan_begin_.push_back((uint32_t)plans_.size());
+        plans_.insert(plans_.end(), ps.begin(), ps.end());
+    }
+    plan_begin_.push_back((uint32_t)plans_.size());
+    std::vector<DevPlan> dplans;
+    std::vector<DevTailTerm> terms;
+    for (auto &hp : plans_) {
+        hp.dev.term_begin = (uint32_t)terms.size();
+        terms.insert(terms.end(), hp.terms.begin(), hp.terms.end());
+        dplans.push_back(hp.dev);
+    }
+    CSM_CUDA(dalloc(&d_plans_, dplans.size()));
+    CSM_CUDA(cudaMemcpy(d_plans_, dplans.data(), sizeof(DevPlan) * dplans.size(), cudaMemcpyHostToDevice));
+    CSM_CUDA(dalloc(&d_terms_, terms.size()));
+    if (!terms.empty())
+        CSM_CUDA(cudaMemcpy(d_terms_, terms.data(), sizeof(DevTailTerm) * terms.size(), cudaMemcpyHostToDevice));
+    const uint32_t np = (uint32_t)plans_.size();
+    CSM_CUDA(dalloc(&d_seed_lo_, 3 * (size_t)np));
+    CSM_CUDA(dalloc(&d_ticket_prefix_, np + 1));
+    CSM_CUDA(dalloc(&d_counts_, 2 * (size_t)np));
+    last_counts_.assign(2 * np, 0);
+    cudaFreeHost(h_counts_);
+    h_counts_ = nullptr;
+    CSM_CUDA(cudaMallocHost(&h_counts_, sizeof(unsigned long long) * (2 * np + 32)));
+    // Donation queue and the semi-BFS frontier.
+    qcap_ = 1u << 20;
+    CSM_CUDA(dalloc(&d_queue_, qcap_));
+    CSM_CUDA(dalloc(&d_ready_, qcap_));
+    CSM_CUDA(cudaMemset(d_ready_, 0, sizeof(uint32_t) * qcap_));
+    const unsigned long long fbytes = cfg_.frontier_bytes ? cfg_.frontier_bytes : (1ull << 30);
+    frontier_cap_ = std::max<unsigned long long>(1024, fbytes / 2 / sizeof(WorkItem));
+    if (opt_.search_strategy >= 2) {
+        CSM_CUDA(dalloc(&d_frontier_[0], frontier_cap_));
+        CSM_CUDA(dalloc(&d_frontier_[1], frontier_cap_));
+    }
+    if (cfg_.materialize_rows) {
+        row_cap_ = cfg_.materialize_rows;
+        CSM_CUDA(dalloc(&d_rows_, row_cap_ * CSM_ROW_WORDS));
+    }
+    csm_status bst = ensure_batch_capacity(cfg_.max_batch ? cfg_.max_batch : 65536);
+    if (bst != CSM_OK) return bst;
+    CSM_CUDA(cudaStreamSynchronize(stream_));
+    CSM_CUDA(cudaGetLastError());
+    unsigned long long top = 0;
+    CSM_CUDA(cudaMemcpy(&top, g_.pool_top, sizeof(top), cudaMemcpyDeviceToHost));
+    stats_.pool_used = top;
+    stats_.pool_capacity = g_.pool_cap;
+    graph_loaded_ = true;
+    return CSM_OK;
+}
+
+csm_status Engine::ensure_batch_capacity(uint64_t n) {
+    if (n <= batch_cap_) return CSM_OK;
+    uint64_t cap = std::max<uint64_t>(n, batch_cap_ * 2);
+    if (2 * cap >= 0x7FFFFFFFull) return fail(CSM_ERR_LIMIT, "batch too large (limit 2^30 updates)");
+    CSM_CUDA(cudaStreamSynchronize(stream_));
+    void *old[] = {d_upd_src_, d_upd_dst_, d_upd_lab_, d_upd_del_, d_keys_raw_, d_keys_, d_sort_temp_, bs_.eff,
+                   bs_.heads, bs_.nheads, bs_.seg_nins, bs_.seg_ndel, bs_.seg_end, bs_.scr_y, bs_.scr_lb, bs_.counters,
+                   bs_.error};
+    for (void *p : old)
+        if (p) cudaFree(p);
+    if (h_pin_) cudaFreeHost(h_pin_);
+    const size_t m = 2 * cap;
+    CSM_CUDA(dalloc(&d_upd_src_, cap));
+    CSM_CUDA(dalloc(&d_upd_dst_, cap));
+    CSM_CUDA(dalloc(&d_upd_lab_, cap));
+    CSM_CUDA(dalloc(&d_upd_del_, cap));
+    CSM_CUDA(cudaMallocHost(&h_pin_, sizeof(uint32_t) * 3 * cap + cap + 64));
+    CSM_CUDA(dalloc(&d_keys_raw_, m));
+    CSM_CUDA(dalloc(&d_keys_, m));
+    sort_temp_bytes_ = 0;
+    store_sort_keys(nullptr, sort_temp_bytes_, d_keys_raw_, d_keys_, (uint32_t)m, kl_, stream_);
+    CSM_CUDA(cudaMalloc(&d_sort_temp_, sort_temp_bytes_ + 16));
+    CSM_CUDA(dalloc(&bs_.eff, m));
+    CSM_CUDA(dalloc(&bs_.heads, m));
+    CSM_CUDA(dalloc(&bs_.nheads, 1));
+    CSM_CUDA(dalloc(&bs_.seg_nins, m));
+    CSM_CUDA(dalloc(&bs_.seg_ndel, m));
+    CSM_CUDA(dalloc(&bs_.seg_end, m));
+    CSM_CUDA(dalloc(&bs_.scr_y, m));
+    CSM_CUDA(dalloc(&bs_.scr_lb, m));
+    CSM_CUDA(dalloc(&bs_.counters, 2));
+    CSM_CUDA(dalloc(&bs_.error, 1));
+    batch_cap_ = cap;
+    return CSM_OK;
+}
+
+csm_status Engine::apply_host(uint64_t n, const uint32_t *src, const uint32_t *dst, const uint32_t *elabel,
+                              const uint8_t *is_delete, csm_batch_result *out) {
+    if (!graph_loaded_) return fail(CSM_ERR_STATE, "load the data graph first");
+    if (poisoned_) return fail(CSM_ERR_STATE, "the engine failed an earlier batch; recreate it");
+    if (n && (!src || !dst || !elabel)) return fail(CSM_ERR_INVALID_ARG, "null update array");
+    csm_status st = ensure_batch_capacity(n);
+    if (st != CSM_OK) return st;
+    bool has_delete = false;
+    if (is_delete)
+        for (uint64_t i = 0; i < n && !has_delete; i++) has_delete = is_delete[i] != 0;
+    // Timed from the first host->device copy (technique_permutation.h:123 includes the H2D).
+    CSM_CUDA(cudaEventRecord(ev_[0], stream_));
+    if (n) {
+        CSM_CUDA(cudaMemcpyAsync(d_upd_src_, src, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, stream_));
+        CSM_CUDA(cudaMemcpyAsync(d_upd_dst_, dst, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, stream_));
+        CSM_CUDA(cudaMemcpyAsync(d_upd_lab_, elabel, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, stream_));
+        if (has_delete)
+            CSM_CUDA(cudaMemcpyAsync(d_upd_del_, is_delete, n, cudaMemcpyHostToDevice, stream_));
+    }
+    return run_batch(n, d_upd_src_, d_upd_dst_, d_upd_lab_, has_delete ? d_upd_del_ : nullptr, has_delete, stream_,
+                     out);
+}
+
+csm_status Engine::apply_device(uint64_t n, const uint32_t *src, const uint32_t *dst, const uint32_t *elabel,
+                                const uint8_t *is_delete, cudaStream_t stream, csm_batch_result *out) {
+    if (!graph_loaded_) return fail(CSM_ERR_STATE, "load the data graph first");
+    if (poisoned_) return fail(CSM_ERR_STATE, "the engine failed an earlier batch; recreate it");
+    if (n && (!src || !dst || !elabel)) return fail(CSM_ERR_INVALID_ARG, "null update array");
+    csm_status st = ensure_batch_capacity(n);
+    if (st != CSM_OK) return st;
+    cudaStream_t s = stream ? stream : stream_;
+    CSM_CUDA(cudaEventRecord(ev_[0], s));
+    return run_batch(n, src, dst, elabel, is_delete, is_delete != nullptr, s, out);
+}
+
+csm_status Engine::run_batch(uint64_t n, const uint32_t *src, const uint32_t *dst, const uint32_t *elabel,
+                             const uint8_t *is_delete, bool has_delete, cudaStream_t s, csm_batch_result *out) {
+    const uint32_t m = (uint32_t)(2 * n);
+    const uint32_t np = (uint32_t)plans_.size();
+    rows_valid_ = false;
+    phase_ran_[0] = phase_ran_[1] = false;
+    CSM_CUDA(cudaMemsetAsync(bs_.nheads, 0, sizeof(unsigned int), s));
+    CSM_CUDA(cudaMemsetAsync(bs_.counters, 0, 2 * sizeof(unsigned long long), s));
+    CSM_CUDA(cudaMemsetAsync(bs_.error, 0, sizeof(unsigned int), s));
+    CSM_CUDA(cudaMemsetAsync(d_counts_, 0, 2 * sizeof(unsigned long long) * np, s));
+    NlfTables nt{d_spec_begin_, d_specs_, d_bits_, words_};
+    if (m) {
+        LabelTables lt{d_elab_raw_, (uint32_t)elab_raw_.size(), d_rel_table_, (uint32_t)vlab_raw_.size()};
+        store_build_keys(n, src, dst, elabel, is_delete, lt, g_, kl_, d_keys_raw_, s);
+        size_t tb = sort_temp_bytes_;
+        CSM_CUDA(store_sort_keys(d_sort_temp_, tb, d_keys_raw_, d_keys_, m, kl_, s));
+        store_classify(m, d_keys_, kl_, g_, bs_, s);
+        stats_.kernel_launches += 3;
+        if (has_delete) {
+            // Destroyed embeddings are counted on the graph before the deletions, with the
+            // deleted edges flagged; then the flagged entries are compacted away.
+            csm_status st = enumerate_phase(CSM_PHASE_DEL, m, s);
+            if (st != CSM_OK) return st;
+            store_delete(m, d_keys_, kl_, g_, bs_, s);
+            stats_.kernel_launches++;
+        }
+        store_insert(m, d_keys_, kl_, g_, bs_, s);
+        store_nlf_update(m, d_keys_, kl_, g_, bs_, nt, s);
+        stats_.kernel_launches += 2;
+        csm_status st = enumerate_phase(CSM_PHASE_INS, m, s);
+        if (st != CSM_OK) return st;
+        store_clear_ins(m, d_keys_, kl_, g_, bs_, s);
+        stats_.kernel_launches++;
+    }
+    unsigned int *h_err = reinterpret_cast<unsigned int *>(h_counts_ + 2 * np + 3);
+    for (int attempt = 0;; attempt++) {
+        CSM_CUDA(cudaEventRecord(ev_[1], s));
+        CSM_CUDA(cudaMemcpyAsync(h_counts_, d_counts_, 2 * sizeof(unsigned long long) * np, cudaMemcpyDeviceToHost, s));
+        CSM_CUDA(cudaMemcpyAsync(h_counts_ + 2 * np, bs_.counters, 2 * sizeof(unsigned long long),
+                                 cudaMemcpyDeviceToHost, s));
+        CSM_CUDA(cudaMemcpyAsync(h_counts_ + 2 * np + 2, g_.pool_top, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                 s));
+        CSM_CUDA(cudaMemcpyAsync(h_err, bs_.error, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+        CSM_CUDA(cudaStreamSynchronize(s));
+        CSM_CUDA(cudaGetLastError());
+        stats_.pool_used = h_counts_[2 * np + 2];
+        if (!(*h_err & CSM_ERRBIT_POOL)) break;
+        if (attempt > 0) {
+            poisoned_ = true;
+            return fail(CSM_ERR_OOM, "adjacency pool exhausted while applying a batch");
+        }
+        // The pool ran out during the merge, and the insertion phase skipped its work: lay the
+        // lists out again in a larger pool, redo the merge (lists already merged are skipped),
+        // the candidate refresh and the insertion phase.
+        stats_.pool_used = g_.pool_cap;
+        csm_status cst = maybe_compact(s);
+        if (cst != CSM_OK) return cst;
+        CSM_CUDA(cudaMemsetAsync(bs_.error, 0, sizeof(unsigned int), s));
+        CSM_CUDA(cudaMemsetAsync(d_counts_ + np, 0, sizeof(unsigned long long) * np, s));
+        store_insert(m, d_keys_, kl_, g_, bs_, s);
+        store_nlf_update(m, d_keys_, kl_, g_, bs_, nt, s);
+        csm_status st = enumerate_phase(CSM_PHASE_INS, m, s);
+        if (st != CSM_OK) return st;
+        store_clear_ins(m, d_keys_, kl_, g_, bs_, s);
+    }
+    float total_ms = 0.f, enum_ms = 0.f;
+    CSM_CUDA(cudaEventElapsedTime(&total_ms, ev_[0], ev_[1]));
+    for (int ph = 0; ph < 2; ph++) {
+        if (!phase_ran_[ph]) continue;
+        float t = 0.f;
+        CSM_CUDA(cudaEventElapsedTime(&t, ev_[2 + 2 * ph], ev_[3 + 2 * ph]));
+        enum_ms += t;
+        const EnumControl &c = h_ctrl_[ph];
+        stats_.enum_scan_entries += c.scan_entries;
+        stats_.enum_probes += c.probes;
+        stats_.enum_tail_lists += c.tail_lists;
+        stats_.donations += c.donations;
+        if (c.error & CSM_ERRBIT_TIMEOUT) return fail(CSM_ERR_TIMEOUT, "enumeration wait bound exceeded");
+        if (c.error & CSM_ERRBIT_OUTPUT) return fail(CSM_ERR_OVERFLOW, "embedding row buffer too small");
+    }
+    for (uint32_t i = 0; i < 2 * np; i++) last_counts_[i] = h_counts_[i];
+    const uint64_t ins = h_counts_[2 * np], del = h_counts_[2 * np + 1];
+    stats_.batches++;
+    stats_.enum_ns += (uint64_t)(enum_ms * 1e6);
+    stats_.apply_ns += (uint64_t)((total_ms - enum_ms) * 1e6);
+    if (out) {
+        for (uint32_t qi = 0; qi < queries_.size(); qi++) {
+            csm_batch_result &r = out[qi];
+            std::memset(&r, 0, sizeof(r));
+            for (uint32_t p = plan_begin_[qi]; p < plan_begin_[qi + 1]; p++) {
+                r.positive += last_counts_[p + np];
+                r.negative += last_counts_[p];
+            }
+            r.inserted = ins;
+            r.deleted = del;
+            r.latency_ns = (uint64_t)(total_ms * 1e6);
+            r.enum_ns = (uint64_t)(enum_ms * 1e6);
+            r.apply_ns = r.latency_ns > r.enum_ns ? r.latency_ns - r.enum_ns : 0;
+        }
+    }
+    if (cfg_.materialize_rows) rows_valid_ = true;
+    return maybe_compact(s);
+}
+
+csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
+    const uint32_t np = (uint32_t)plans_.size();
+    const uint32_t total_warps = (uint32_t)(blocks_ * warps_per_block_);
+    EnumParams P{};
+    P.plans = d_plans_;
+    P.nplans = np;
+    P.terms = d_terms_;
+    P.g = g_.view();
+    P.bits = d_bits_;
+    P.words = words_;
+    P.keys = d_keys_;
+    P.m = m;
+    P.kl = kl_;
+    P.eff = bs_.eff;
+    P.seg_flagged = phase == CSM_PHASE_INS ? bs_.seg_nins : bs_.seg_ndel;
+    P.phase = phase;
+    P.seed_lo = d_seed_lo_;
+    P.ticket_prefix = d_ticket_prefix_;
+    P.queue = d_queue_;
+    P.ready = d_ready_;
+    P.qcap = qcap_;
+    P.ctrl = d_ctrl_;
+    P.counts = d_counts_ + (phase == CSM_PHASE_INS ? np : 0);
+    P.steal_min = cfg_.steal_chunk > 0 ? (uint32_t)cfg_.steal_chunk : 64u;
+    P.idle_limit = 1u << 18;
+    P.abort_flag = phase == CSM_PHASE_INS ? bs_.error : nullptr;
+    P.rows = d_rows_;
+    P.row_cap = row_cap_;
+    const bool rows = cfg_.materialize_rows > 0;
+    const int strategy = opt_.search_strategy;
+    const int ph = phase == CSM_PHASE_INS ? 1 : 0;
+    phase_ran_[ph] = true;
+    CSM_CUDA(cudaEventRecord(ev_[2 + 2 * ph], s));
+
+    launch_ctrl_reset(d_ctrl_, total_warps, ++epoch_, 0, s);
+    launch_seed_tickets(d_plans_, np, d_keys_, m, kl_, d_seed_lo_, d_ticket_prefix_, d_ctrl_, s);
+    stats_.kernel_launches += 3;
+    const WorkItem *frontier = nullptr;
+    unsigned long long nfront = 0;
+    if (strategy >= 2 && !rows) {
+        // Semi-BFS (Matching / BfsMatching, match_gpu.cu:1916-2294): expand levels while the
+        // frontier is small (strategy 2) or while it fits the budget (strategy 3); the size of
+        // the next level is bounded from list sizes before it is written, so a level that would
+        // not fit is never started and the search continues depth first from the current one.
+        CSM_CUDA(cudaMemcpyAsync(h_counts_ + 2 * np + 4, &d_ctrl_->nticket, sizeof(unsigned long long),
+                                 cudaMemcpyDeviceToHost, s));
+        CSM_CUDA(cudaStreamSynchronize(s));
+        unsigned long long cur = h_counts_[2 * np + 4] * 32;  // seed candidates (upper bound)
+        const unsigned long long target = 8ull * total_warps;
+        int buf = 0;
+        for (int level = 0; level < CSM_MAXQV; level++) {
+            if (strategy == 2 && cur >= target) break;
+            if (cur == 0) break;
+            unsigned long long bound = cur;
+            if (frontier) {
+                h_counts_[2 * np + 4] = nfront;
+                CSM_CUDA(cudaMemcpyAsync(d_misc_, h_counts_ + 2 * np + 4, 8, cudaMemcpyHostToDevice, s));
+                CSM_CUDA(cudaMemsetAsync(&d_ctrl_->expand_bound, 0, 8, s));
+                launch_expand_bound(P, frontier, d_misc_, s);
+                CSM_CUDA(cudaMemcpyAsync(h_counts_ + 2 * np + 5, &d_ctrl_->expand_bound, 8, cudaMemcpyDeviceToHost, s));
+                CSM_CUDA(cudaStreamSynchronize(s));
+                bound = h_counts_[2 * np + 5];
+            }
+            if (bound > frontier_cap_) break;
+            EnumParams X = P;
+            X.mode = CSM_ENUM_MODE_EXPAND;
+            X.donate = 0;
+            X.frontier = frontier;
+            X.expand_out = d_frontier_[buf];
+            X.expand_cap = frontier_cap_;
+            if (frontier) launch_ctrl_reset(d_ctrl_, total_warps, ++epoch_, nfront, s);
+            launch_enumerate(X, blocks_, warps_per_block_, s);
+            stats_.enum_launches++;
+            stats_.kernel_launches++;
+            CSM_CUDA(cudaMemcpyAsync(&h_ctrl_[ph], d_ctrl_, sizeof(EnumControl), cudaMemcpyDeviceToHost, s));
+            CSM_CUDA(cudaStreamSynchronize(s));
+            const unsigned long long rows_out = h_ctrl_[ph].out_rows;
+            const unsigned int errb = h_ctrl_[ph].error;
+            if (errb & CSM_ERRBIT_OUTPUT) return fail(CSM_ERR_OVERFLOW, "semi-BFS frontier overflow");
+            const bool grew = rows_out != nfront || frontier == nullptr;
+            frontier = d_frontier_[buf];
+            nfront = rows_out;
+            buf ^= 1;
+            cur = nfront;
+            if (!grew) break;
+        }
+    }
+    EnumParams D = P;
+    D.mode = rows ? CSM_ENUM_MODE_ROWS : CSM_ENUM_MODE_COUNT;
+    D.donate = (strategy == 0 || strategy == 2) ? 1u : 0u;
+    if (frontier) {
+        D.frontier = frontier;
+        launch_ctrl_reset(d_ctrl_, total_warps, ++epoch_, nfront, s);
+        stats_.kernel_launches++;
+    }
+    launch_enumerate(D, blocks_, warps_per_block_, s);
+    stats_.enum_launches++;
+    stats_.kernel_launches++;
+    CSM_CUDA(cudaEventRecord(ev_[3 + 2 * ph], s));
+    // Statistics and error bits are read after the batch's final synchronisation.
+    CSM_CUDA(cudaMemcpyAsync(&h_ctrl_[ph], d_ctrl_, sizeof(EnumControl), cudaMemcpyDeviceToHost, s));
+    if (rows) {
+        // Collect rows per query for csm_get_embeddings (a validation path: synchronous).
+        CSM_CUDA(cudaStreamSynchronize(s));
+        const EnumControl &c = h_ctrl_[ph];
+        if (c.error & CSM_ERRBIT_OUTPUT) return fail(CSM_ERR_OVERFLOW, "embedding row buffer too small");
+        const unsigned long long nr = c.out_rows;
+        std::vector<uint32_t> h(nr * CSM_ROW_WORDS);
+        if (nr) CSM_CUDA(cudaMemcpy(h.data(), d_rows_, sizeof(uint32_t) * h.size(), cudaMemcpyDeviceToHost));
+        auto &dst = last_rows_[phase == CSM_PHASE_INS ? 0 : 1];
+        dst.assign(queries_.size(), {});
+        for (unsigned long long r = 0; r < nr; r++) {
+            const uint32_t *row = &h[r * CSM_ROW_WORDS];
+            const uint32_t qi = row[0];
+            dst[qi].insert(dst[qi].end(), row + 1, row + 1 + queries_[qi].nv);
+        }
+    }
+    return CSM_OK;
+}
+
+csm_status Engine::maybe_compact(cudaStream_t s) {
+    const unsigned long long used = stats_.pool_used;
+    const uint64_t max_batch = batch_cap_ ? batch_cap_ : 65536;
+    const unsigned long long headroom = 64ull * max_batch + (1u << 20);
+    if (used + headroom < g_.pool_cap && used < g_.pool_cap / 4 * 3) return CSM_OK;
+    // Lay every list out again with fresh slack; grow the pool when the live lists need it.
+    unsigned long long new_cap = g_.pool_cap;
+    for (int attempt = 0; attempt < 4; attempt++) {
+        uint32_t *np = nullptr;
+        cudaError_t e = cudaMalloc(&np, sizeof(uint32_t) * new_cap);
+        if (e != cudaSuccess) return cuda_fail(e, "pool compaction");
+        unsigned long long live = 0;
+        e = store_compact(g_, np, new_cap, s, live);
+        if (e == cudaSuccess && live + headroom < new_cap && live < new_cap / 4 * 3) {
+            cudaFree(g_.pool);
+            g_.pool = np;
+            g_.pool_cap = new_cap;
+            stats_.pool_used = live;
+            stats_.pool_capacity = new_cap;
+            stats_.compactions++;
+            return CSM_OK;
+        }
+        cudaFree(np);
+        if (e != cudaSuccess && e != cudaErrorMemoryAllocation) return cuda_fail(e, "pool compaction");
+        if (e == cudaSuccess) {
+            // The layout fit but left too little headroom: keep it only if growth is impossible.
+            new_cap = std::min<unsigned long long>(0xFFFFFFF0ull, std::max(new_cap * 2, 2 * (live + headroom)));
+        } else {
+            new_cap = std::min<unsigned long long>(0xFFFFFFF0ull, new_cap * 2);
+        }
+    }
+    return fail(CSM_ERR_OOM, "adjacency pool cannot grow further");
+}
+
+csm_status Engine::edge_counts(int32_t qid, uint64_t *pos, uint64_t *neg, uint32_t capacity, uint32_t *n_out) const {
+    if (qid < 0 || qid >= (int32_t)queries_.size()) return CSM_ERR_INVALID_ARG;
+    if (!graph_loaded_) return CSM_ERR_STATE;
+    const uint32_t np = (uint32_t)plans_.size();
+    const uint32_t b = plan_begin_[qid], e = plan_begin_[qid + 1];
+    if (n_out) *n_out = e - b;
+    for (uint32_t p = b; p < e && p - b < capacity; p++) {
+        if (pos) pos[p - b] = last_counts_[p + np];
+        if (neg) neg[p - b] = last_counts_[p];
+    }
+    return CSM_OK;
+}
+
+csm_status Engine::embeddings(int32_t qid, int32_t sign, uint32_t **rows, uint64_t *nrows) {
+    if (qid < 0 || qid >= (int32_t)queries_.size() || !rows || !nrows)
+        return fail(CSM_ERR_INVALID_ARG, "bad embeddings arguments");
+    if (!cfg_.materialize_rows) return fail(CSM_ERR_STATE, "rows are kept only with materialize_rows > 0");
+    if (!rows_valid_) return fail(CSM_ERR_STATE, "no batch has been applied");
+    const auto &src = last_rows_[sign >= 0 ? 0 : 1];
+    const uint32_t nv = queries_[qid].nv;
+    std::vector<uint32_t> flat = qid < (int32_t)src.size() ? src[qid] : std::vector<uint32_t>();
+    const uint64_t nr = flat.size() / nv;
+    std::vector<uint64_t> idx(nr);
+    for (uint64_t i = 0; i < nr; i++) idx[i] = i;
+    std::sort(idx.begin(), idx.end(), [&](uint64_t a, uint64_t b) {
+        return std::lexicographical_compare(flat.begin() + a * nv, flat.begin() + (a + 1) * nv, flat.begin() + b * nv,
+                                            flat.begin() + (b + 1) * nv);
+    });
+    uint32_t *outp = (uint32_t *)malloc(sizeof(uint32_t) * (nr * nv + 1));
+    if (!outp) return fail(CSM_ERR_OOM, "host allocation for rows");
+    for (uint64_t i = 0; i < nr; i++) std::memcpy(outp + i * nv, flat.data() + idx[i] * nv, sizeof(uint32_t) * nv);
+    *rows = outp;
+    *nrows = nr;
+    return CSM_OK;
+}
+
+csm_status Engine::describe(int32_t qid, char *buf, size_t n) const {
+    if (qid < 0 || qid >= (int32_t)queries_.size() || !buf || n == 0) return CSM_ERR_INVALID_ARG;
+    if (!graph_loaded_) return CSM_ERR_STATE;
+    std::vector<HostPlan> ps(plans_.begin() + plan_begin_[qid], plans_.begin() + plan_begin_[qid + 1]);
+    std::string s = describe_plans(queries_[qid], ps);
+    std::snprintf(buf, n, "%s", s.c_str());
+    return CSM_OK;
+}
+
+csm_status Engine::stats(csm_stats *out) const {
+    if (!out) return CSM_ERR_INVALID_ARG;
+    *out = stats_;
+    return CSM_OK;
+}
+
+void Engine::reset_stats() {
+    const uint64_t used = stats_.pool_used, cap = stats_.pool_capacity;
+    std::memset(&stats_, 0, sizeof(stats_));
+    stats_.pool_used = used;
+    stats_.pool_capacity = cap;
+}
+
+csm_status Engine::memory(uint64_t *free_b, uint64_t *total_b) const {
+    size_t f = 0, t = 0;
+    cudaError_t e = cudaMemGetInfo(&f, &t);
+    if (e != cudaSuccess) return CSM_ERR_CUDA;
+    if (free_b) *free_b = f;
+    if (total_b) *total_b = t;
+    return CSM_OK;
+}
+
+}  // namespace csm

@@ -1,0 +1,140 @@
+// The engine behind the C ABI: owns the device graph, the candidate bitmaps, the plans and
+// the per-batch scratch of one GPU.  Replaces class MatchGPU (graph/match_gpu.h:80-225) and the
+// batch loop of TechniquePermutationProcess (technique_permutation.h:121-214).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/csm.h"
+#include "common.h"
+#include "kernels.cuh"
+#include "plan.h"
+#include "query.h"
+#include "store.cuh"
+
+namespace csm {
+
+struct Options {
+    Order order = Order::kGcsm;
+    int search_strategy = 2;  // 0 DFS+stealing, 1 DFS, 2 dynamic BFS-DFS, 3 BFS
+    bool local_index = true;
+    bool cartesian = true;
+    bool heavy_vertex_avoidance = true;
+    bool relation_switch = true;
+};
+
+// Resolves --algorithm presets (utils/technique_option.h:58-86).
+Options resolve_options(const csm_config &cfg);
+
+class Engine {
+  public:
+    explicit Engine(const csm_config &cfg);
+    ~Engine();
+
+    csm_status init();
+    csm_status load_query(uint32_t nv, const uint32_t *vlabel, uint32_t ne, const uint32_t *src, const uint32_t *dst,
+                          const uint32_t *elabel, int32_t *qid);
+    csm_status load_graph(uint32_t nv, const uint32_t *vlabel, uint64_t ne, const uint32_t *src, const uint32_t *dst,
+                          const uint32_t *elabel);
+    csm_status apply_host(uint64_t n, const uint32_t *src, const uint32_t *dst, const uint32_t *elabel,
+                          const uint8_t *is_delete, csm_batch_result *out);
+    csm_status apply_device(uint64_t n, const uint32_t *src, const uint32_t *dst, const uint32_t *elabel,
+                            const uint8_t *is_delete, cudaStream_t stream, csm_batch_result *out);
+    csm_status edge_counts(int32_t qid, uint64_t *pos, uint64_t *neg, uint32_t capacity, uint32_t *n_out) const;
+    csm_status embeddings(int32_t qid, int32_t sign, uint32_t **rows, uint64_t *nrows);
+    csm_status describe(int32_t qid, char *buf, size_t n) const;
+    csm_status stats(csm_stats *out) const;
+    void reset_stats();
+    csm_status memory(uint64_t *free_b, uint64_t *total_b) const;
+
+    const std::string &error() const { return err_; }
+    csm_status fail(csm_status code, const std::string &msg);
+    csm_status cuda_fail(cudaError_t e, const char *where);
+
+    uint32_t num_queries() const { return (uint32_t)queries_.size(); }
+
+  private:
+    csm_status ensure_batch_capacity(uint64_t n);
+    csm_status run_batch(uint64_t n, const uint32_t *src, const uint32_t *dst, const uint32_t *elabel,
+                         const uint8_t *is_delete, bool has_delete, cudaStream_t s, csm_batch_result *out);
+    csm_status enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s);
+    csm_status maybe_compact(cudaStream_t s);
+
+    csm_config cfg_;
+    Options opt_;
+    std::string err_;
+    int device_ = 0;
+    int sm_count_ = 148;
+    bool graph_loaded_ = false;
+    bool poisoned_ = false;
+    cudaStream_t stream_ = nullptr;
+    cudaEvent_t ev_[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // batch, DEL enum, INS enum
+
+    // Queries and label spaces.
+    std::vector<Query> queries_;
+    std::vector<uint32_t> vlab_raw_;      // sorted raw vertex labels of all queries
+    std::vector<uint32_t> elab_raw_;      // sorted raw edge labels of all queries
+    std::vector<uint32_t> rel_triples_;   // rel -> (a << 16 | l << 8 | b)
+    std::vector<uint16_t> rel_table_;     // host copy of the device table
+    std::vector<uint32_t> nlf_base_;      // first bitmap of each query
+
+    // Device tables.
+    uint32_t *d_elab_raw_ = nullptr;
+    uint16_t *d_rel_table_ = nullptr;
+    uint32_t *d_spec_begin_ = nullptr;
+    NlfSpec *d_specs_ = nullptr;
+    uint32_t *d_bits_ = nullptr;
+    uint32_t nbitmaps_ = 0;
+    uint32_t words_ = 0;
+    DeviceGraph g_;
+    KeyLayout kl_{};
+
+    // Plans.
+    std::vector<HostPlan> plans_;
+    std::vector<uint32_t> plan_begin_;    // per query, first plan (plus one past the end)
+    DevPlan *d_plans_ = nullptr;
+    DevTailTerm *d_terms_ = nullptr;
+
+    // Batch buffers.
+    uint64_t batch_cap_ = 0;              // updates
+    uint32_t *d_upd_src_ = nullptr, *d_upd_dst_ = nullptr, *d_upd_lab_ = nullptr;
+    uint8_t *d_upd_del_ = nullptr;
+    uint32_t *h_pin_ = nullptr;           // pinned staging: src, dst, lab (3 * cap) + del bytes
+    unsigned long long *d_keys_raw_ = nullptr, *d_keys_ = nullptr;
+    void *d_sort_temp_ = nullptr;
+    size_t sort_temp_bytes_ = 0;
+    BatchScratch bs_;
+
+    // Enumeration state.
+    EnumControl *d_ctrl_ = nullptr;
+    WorkItem *d_queue_ = nullptr;
+    uint32_t *d_ready_ = nullptr;
+    uint32_t qcap_ = 0;
+    uint32_t epoch_ = 0;
+    uint32_t *d_seed_lo_ = nullptr;       // 3 * nplans
+    uint32_t *d_ticket_prefix_ = nullptr; // nplans + 1
+    unsigned long long *d_counts_ = nullptr;  // per plan, per phase (2 * nplans)
+    WorkItem *d_frontier_[2] = {nullptr, nullptr};
+    unsigned long long frontier_cap_ = 0;
+    uint32_t *d_rows_ = nullptr;
+    unsigned long long row_cap_ = 0;
+    unsigned long long *h_counts_ = nullptr;  // pinned readback
+    EnumControl *h_ctrl_ = nullptr;           // pinned: control block of the DEL and INS launches
+    unsigned long long *d_misc_ = nullptr;    // small device scratch
+    bool phase_ran_[2] = {false, false};
+    int warps_per_block_ = 8;
+    int blocks_ = 0;
+
+    // Results of the last batch.
+    std::vector<uint64_t> last_counts_;   // 2 * nplans
+    std::vector<std::vector<uint32_t>> last_rows_[2];  // per phase, per query: flattened rows
+    bool rows_valid_ = false;
+
+    csm_stats stats_{};
+};
+
+}  // namespace csm

@@ -1,0 +1,748 @@
+// Persistent warp-DFS enumeration of incremental matches.
+//
+// Replaces the reference's enumeration kernels: write_initial_partial_results
+// (kernels/enumeration.cu:24-79), extendBFSDFSRegTwo (enumeration.cu:407-781),
+// gamma_enumerate with its work stealing (kernels/gamma_enumeration.cu:209-880) and the
+// Cartesian-product flattening GetNumTree / enumerateCartesianProductTree
+// (kernels/cartesian_product.cu:193-284).
+//
+// One launch covers every (query, updated query edge) plan of a batch.  A warp owns one work
+// item at a time and walks its subtree depth first: at each level the candidates are the
+// entries of the smallest backward-neighbour list (the pivot), filtered 32 at a time by the
+// lanes (flag rule, NLF bitmap, injectivity, membership in the other backward lists by binary
+// search) and compacted with ballot/popc into a per-level shared-memory buffer.
+//
+// Counting rule of the per-query-edge decomposition (technique_permutation.h:125-212): for the
+// plan of query edge i the starting edge is a batch edge; an edge matched to a query edge with
+// index > i must not be a batch edge; edges of query edges < i may be either.  Every new
+// embedding is counted exactly once, at the largest query-edge index it maps to a batch edge.
+//
+// Load balance: warps first take seed chunks from a ticket counter.  A warp that runs out of
+// work registers as hungry; busy warps that see hungry warps split off part of their pending
+// work (the upper half of a candidate range, or buffered sibling candidates) into a global
+// queue.  Every wait is bounded; a warp never waits on another warp's progress to finish its
+// own items, so exhausting a bound only costs balance, never a result.
+//
+// Tail leaves (query vertices of degree one matched after their neighbour) are not enumerated:
+// their number of injective assignments is computed from list sizes by inclusion-exclusion.
+#include <cuda_runtime.h>
+
+#include "kernels.cuh"
+
+namespace csm {
+
+namespace {
+
+struct __align__(16) WarpState {
+    uint32_t f[CSM_MAXQV];
+    uint32_t buf[CSM_MAXQV][CSM_WARP];
+    uint32_t lo[CSM_MAXQV];
+    uint32_t hi[CSM_MAXQV];
+    uint32_t base[CSM_MAXQV];
+    uint32_t poff[CSM_MAXQV][CSM_MAXBN];
+    uint32_t psz[CSM_MAXQV][CSM_MAXBN];
+    uint32_t nlf[CSM_MAXQV];
+    uint16_t oldm[CSM_MAXQV];
+    uint8_t nbuf[CSM_MAXQV];
+    uint8_t pos[CSM_MAXQV];
+    uint8_t piv[CSM_MAXQV];
+    uint8_t nbn[CSM_MAXQV];
+    uint32_t t_off[CSM_TAIL_MAXKEYS];
+    uint32_t t_size[CSM_TAIL_MAXKEYS];
+    uint32_t t_flag[CSM_TAIL_MAXKEYS];
+    uint32_t t_excl[CSM_TAIL_MAXKEYS];
+    unsigned long long msize[CSM_TAIL_MAXMASKS];
+    uint32_t item_plan;
+    uint32_t item_depth;
+    uint32_t item_lo;
+    uint32_t item_hi;
+};
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+__device__ __forceinline__ uint32_t warp_min_index(uint32_t v, uint32_t lane) {
+    // Returns the lane holding the smallest v (smallest lane on ties).
+    unsigned long long key = ((unsigned long long)v << 5) | lane;
+    for (int o = 16; o > 0; o >>= 1) {
+        unsigned long long other = __shfl_xor_sync(0xffffffffu, key, o);
+        key = other < key ? other : key;
+    }
+    return (uint32_t)(key & 31u);
+}
+
+__device__ __forceinline__ const uint32_t *bitmap(const EnumParams &P, uint32_t id) {
+    return P.bits + (size_t)id * P.words;
+}
+
+// Sets up level d for the current prefix: the backward-neighbour lists and the pivot.
+__device__ void enter_level(WarpState &S, const EnumParams &P, const DevPlan *pl, uint32_t d, uint32_t rlo,
+                            uint32_t rhi) {
+    const uint32_t lane = lane_id();
+    const DevLevel *lv = &pl->lv[d];
+    const uint32_t nbn = __ldg(&lv->nbn);
+    uint32_t sz = 0xFFFFFFFFu;
+    if (lane < nbn) {
+        const uint32_t rel = __ldg(&lv->bn_rel[lane]);
+        const uint32_t dep = __ldg(&lv->bn_depth[lane]);
+        const uint32_t v = S.f[dep];
+        const uint2 ms = __ldg(P.g.meta + (size_t)rel * P.g.V + v);
+        S.poff[d][lane] = ms.x;
+        S.psz[d][lane] = ms.y;
+        sz = ms.y;
+    }
+    const uint32_t piv = warp_min_index(sz, lane);
+    __syncwarp();
+    if (lane == 0) {
+        S.piv[d] = (uint8_t)piv;
+        S.nbn[d] = (uint8_t)nbn;
+        S.base[d] = S.poff[d][piv];
+        const uint32_t psize = S.psz[d][piv];
+        S.lo[d] = rlo;
+        S.hi[d] = rhi < psize ? rhi : psize;
+        S.nbuf[d] = 0;
+        S.pos[d] = 0;
+        S.oldm[d] = __ldg(&lv->old_mask);
+        S.nlf[d] = __ldg(&lv->nlf_bitmap);
+    }
+    __syncwarp();
+}
+
+// Number of injective assignments of the tail leaves for the full prefix f[0..E-1].
+__device__ unsigned long long tail_count(WarpState &S, const EnumParams &P, const DevPlan *pl,
+                                         unsigned long long &probes) {
+    const uint32_t lane = lane_id();
+    const DevTail *T = &pl->tail;
+    const uint32_t nkeys = __ldg(&T->nkeys);
+    const uint32_t E = pl->tail_start;
+    if (lane < nkeys) {
+        const uint32_t rel = __ldg(&T->key_rel[lane]);
+        const uint32_t x = S.f[__ldg(&T->key_parent[lane])];
+        const uint2 ms = __ldg(P.g.meta + (size_t)rel * P.g.V + x);
+        S.t_off[lane] = ms.x;
+        S.t_size[lane] = ms.y;
+        uint32_t fc = 0;
+        if (__ldg(&T->key_old[lane])) {
+            // Flagged entries of this list = batch edges of (rel, x) in this phase.
+            const unsigned long long lk = P.kl.list_key(rel, x);
+            const uint32_t h = find_list_head(P.keys, P.m, P.kl, lk);
+            if (h < P.m && P.kl.list_of(__ldg(P.keys + h)) == lk) fc = __ldg(P.seg_flagged + h);
+        }
+        S.t_flag[lane] = fc;
+        S.t_excl[lane] = 0;
+    }
+    __syncwarp();
+    // Prefix vertices that sit in a tail list are not available to the leaves.
+    for (uint32_t pi = lane; pi < nkeys * E; pi += 32) {
+        const uint32_t k = pi / E;
+        const uint32_t z = S.f[pi % E];
+        const uint32_t e = find_entry(P.g.pool + S.t_off[k], S.t_size[k], z);
+        if (e != 0xFFFFFFFFu && !(__ldg(&T->key_old[k]) && (e & 1u))) atomicAdd(&S.t_excl[k], 1u);
+    }
+    if (lane == 0) probes += nkeys * E;
+    __syncwarp();
+    const uint32_t nmasks = __ldg(&T->nmasks);
+    for (uint32_t mi = 0; mi < nmasks; mi++) {
+        const uint32_t mask = __ldg(&T->mask[mi]);
+        unsigned long long size;
+        if (__popc(mask) == 1) {
+            const uint32_t k = __ffs(mask) - 1;
+            size = (unsigned long long)S.t_size[k] - S.t_flag[k] - S.t_excl[k];
+        } else {
+            // Intersection of several lists: scan the smallest, probe the others.
+            uint32_t k0 = 0, best = 0xFFFFFFFFu;
+            for (uint32_t k = 0; k < nkeys; k++)
+                if (((mask >> k) & 1u) && S.t_size[k] < best) {
+                    best = S.t_size[k];
+                    k0 = k;
+                }
+            const bool old0 = __ldg(&T->key_old[k0]) != 0;
+            uint32_t cnt = 0;
+            for (uint32_t base = 0; base < best; base += 32) {
+                const uint32_t idx = base + lane;
+                bool ok = idx < best;
+                uint32_t w = 0;
+                if (ok) {
+                    const uint32_t e = __ldg(P.g.pool + S.t_off[k0] + idx);
+                    w = e >> 1;
+                    ok = !(old0 && (e & 1u));
+                }
+                for (uint32_t z = 0; ok && z < E; z++) ok = S.f[z] != w;
+                for (uint32_t k = 0; ok && k < nkeys; k++) {
+                    if (k == k0 || !((mask >> k) & 1u)) continue;
+                    const uint32_t e = find_entry(P.g.pool + S.t_off[k], S.t_size[k], w);
+                    ok = e != 0xFFFFFFFFu && !(__ldg(&T->key_old[k]) && (e & 1u));
+                    probes++;
+                }
+                cnt += __popc(__ballot_sync(0xffffffffu, ok));
+            }
+            size = cnt;
+        }
+        if (lane == 0) S.msize[mi] = size;
+    }
+    __syncwarp();
+    unsigned long long total = 0;
+    if (lane == 0) {
+        total = 1;
+        const DevTailTerm *terms = P.terms + pl->term_begin;
+        const uint32_t nclasses = __ldg(&T->nclasses);
+        for (uint32_t c = 0; c < nclasses; c++) {
+            unsigned long long s = 0;
+            const uint32_t tb = __ldg(&T->class_term_begin[c]), te = __ldg(&T->class_term_begin[c + 1]);
+            for (uint32_t t = tb; t < te; t++) {
+                unsigned long long prod = (unsigned long long)__ldg(&terms[t].coef);
+                const uint32_t nf = __ldg(&terms[t].nf);
+                for (uint32_t j = 0; j < nf; j++) prod *= S.msize[__ldg(&terms[t].f[j])];
+                s += prod;
+            }
+            total *= s;
+        }
+    }
+    __syncwarp();
+    return total;
+}
+
+// Reserves `cnt` queue slots; returns the first slot or 0xFFFFFFFF when the queue is full.
+// Slots that were reserved past a failed reservation are filled with null items.
+__device__ uint32_t reserve_slots(const EnumParams &P, uint32_t cnt) {
+    const uint32_t lane = lane_id();
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(&P.ctrl->q_write, cnt);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base + cnt <= P.qcap) return base;
+    // Mark the reachable part as null so that consumers skip it.
+    for (uint32_t s = base; s < P.qcap && s < base + cnt; s++) {
+        if (lane == 0) {
+            P.queue[s].depth = 0xFFFFFFFFu;
+            __threadfence();
+            atomicExch(P.ready + s, P.ctrl->epoch);
+        }
+    }
+    __syncwarp();
+    return 0xFFFFFFFFu;  // a full queue only costs balance: the donor keeps the work
+}
+
+__device__ void publish_item(const EnumParams &P, uint32_t slot, uint32_t plan, uint32_t depth, uint32_t lo,
+                             uint32_t hi, const uint32_t *prefix, uint32_t nprefix, bool extra, uint32_t extra_v,
+                             uint32_t extra_pos) {
+    const uint32_t lane = lane_id();
+    WorkItem *it = P.queue + slot;
+    if (lane == 0) {
+        it->plan = plan;
+        it->depth = depth;
+        it->lo = lo;
+        it->hi = hi;
+    }
+    if (lane < nprefix) it->f[lane] = prefix[lane];
+    if (extra && lane == 0) it->f[extra_pos] = extra_v;
+    __threadfence();
+    __syncwarp();
+    if (lane == 0) atomicExch(P.ready + slot, P.ctrl->epoch);
+    __syncwarp();
+}
+
+// Splits pending work of the current item into the queue.  Returns true if it donated.
+__device__ bool try_donate(WarpState &S, const EnumParams &P, const DevPlan *pl, uint32_t L0, uint32_t d) {
+    const uint32_t lane = lane_id();
+    const uint32_t E = pl->tail_start;
+    for (uint32_t l = L0; l <= d; l++) {
+        const uint32_t lo = S.lo[l], hi = S.hi[l];
+        const uint32_t minr = (l == 1) ? 64u : P.steal_min;
+        if (hi > lo && hi - lo >= minr) {
+            uint32_t mid = lo + ((hi - lo) >> 1);
+            if (l == 1) mid = (mid + 31u) & ~31u;
+            if (mid >= hi) continue;
+            const uint32_t slot = reserve_slots(P, 1);
+            if (slot == 0xFFFFFFFFu) return false;
+            publish_item(P, slot, S.item_plan, l == 1 ? 0u : l, mid, hi, S.f, l == 1 ? 0u : l, false, 0, 0);
+            if (lane == 0) S.hi[l] = mid;
+            __syncwarp();
+            return true;
+        }
+        const uint32_t nb = S.nbuf[l], ps = S.pos[l];
+        if (l < d && l + 1 < E && nb > ps) {
+            const uint32_t cnt = nb - ps;
+            const uint32_t slot = reserve_slots(P, cnt);
+            if (slot == 0xFFFFFFFFu) return false;
+            for (uint32_t j = 0; j < cnt; j++) {
+                const uint32_t c = S.buf[l][ps + j];
+                if (l == 1) {
+                    const unsigned long long key = __ldg(P.keys + c);
+                    uint32_t pre[2] = {P.kl.src(key), P.kl.dst(key)};
+                    publish_item(P, slot + j, S.item_plan, 2, 0, 0xFFFFFFFFu, pre, 2, false, 0, 0);
+                } else {
+                    publish_item(P, slot + j, S.item_plan, l + 1, 0, 0xFFFFFFFFu, S.f, l, true, c, l);
+                }
+            }
+            if (lane == 0) S.nbuf[l] = (uint8_t)ps;
+            __syncwarp();
+            return true;
+        }
+    }
+    return false;
+}
+
+// Claims one donated item into S; returns 1 on success, 0 if the queue is empty.
+__device__ int claim_item(WarpState &S, const EnumParams &P, unsigned int &err) {
+    const uint32_t lane = lane_id();
+    uint32_t slot = 0xFFFFFFFFu;
+    if (lane == 0) {
+        volatile unsigned int *qr = &P.ctrl->q_read;
+        volatile unsigned int *qw = &P.ctrl->q_write;
+        for (int tries = 0; tries < 256; tries++) {
+            const unsigned int r = *qr;
+            unsigned int w = *qw;
+            if (w > P.qcap) w = P.qcap;
+            if (r >= w) break;
+            if (atomicCAS(&P.ctrl->q_read, r, r + 1) == r) {
+                slot = r;
+                break;
+            }
+        }
+        if (slot != 0xFFFFFFFFu) {
+            volatile uint32_t *rd = P.ready + slot;
+            const uint32_t ep = P.ctrl->epoch;
+            unsigned int spins = 0;
+            while (*rd != ep) {
+                if (++spins > P.idle_limit) {
+                    err |= CSM_ERRBIT_TIMEOUT;
+                    slot = 0xFFFFFFFEu;
+                    break;
+                }
+                __nanosleep(64);
+            }
+            __threadfence();
+        }
+    }
+    slot = __shfl_sync(0xffffffffu, slot, 0);
+    if (slot >= 0xFFFFFFFEu) return 0;
+    volatile const WorkItem *it = P.queue + slot;
+    if (lane == 0) {
+        S.item_plan = it->plan;
+        S.item_depth = it->depth;
+        S.item_lo = it->lo;
+        S.item_hi = it->hi;
+    }
+    if (lane < CSM_MAXQV) S.f[lane] = it->f[lane];
+    __syncwarp();
+    if (S.item_depth == 0xFFFFFFFFu) return -1;  // null slot
+    return 1;
+}
+
+__device__ bool take_ticket(WarpState &S, const EnumParams &P) {
+    const uint32_t lane = lane_id();
+    unsigned long long t = 0;
+    if (lane == 0) t = atomicAdd(&P.ctrl->ticket, 1ull);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    const unsigned long long nt = *(volatile unsigned long long *)&P.ctrl->nticket;
+    if (t >= nt) return false;
+    if (P.frontier != nullptr) {
+        const WorkItem *it = P.frontier + t;
+        if (lane == 0) {
+            S.item_plan = it->plan;
+            S.item_depth = it->depth;
+            S.item_lo = it->lo;
+            S.item_hi = it->hi;
+        }
+        if (lane < CSM_MAXQV) S.f[lane] = it->f[lane];
+    } else {
+        // Seed chunk t: plan p with ticket_prefix[p] <= t < ticket_prefix[p+1].
+        uint32_t lo = 0, hi = P.nplans;
+        while (lo + 1 < hi) {
+            uint32_t mid = (lo + hi) >> 1;
+            if (__ldg(P.ticket_prefix + mid) <= t) lo = mid;
+            else hi = mid;
+        }
+        const uint32_t p = lo;
+        const uint32_t chunk = (uint32_t)(t - __ldg(P.ticket_prefix + p));
+        const uint32_t s0 = __ldg(P.seed_lo + p) + chunk * 32u;
+        const uint32_t s_end = __ldg(P.seed_lo + P.nplans + p);
+        if (lane == 0) {
+            S.item_plan = p;
+            S.item_depth = 0;
+            S.item_lo = s0;
+            S.item_hi = s0 + 32u < s_end ? s0 + 32u : s_end;
+        }
+    }
+    __syncwarp();
+    return true;
+}
+
+__device__ void write_row(const EnumParams &P, const DevPlan *pl, const WarpState &S, uint32_t d, uint32_t w,
+                          unsigned long long r) {
+    uint32_t *row = P.rows + r * CSM_ROW_WORDS;
+    row[0] = pl->query;
+    for (uint32_t k = 0; k < d; k++) row[1 + pl->order[k]] = S.f[k];
+    row[1 + pl->order[d]] = w;
+}
+
+// Runs one work item to completion.  Returns the number of matches counted.
+__device__ unsigned long long run_item(WarpState &S, const EnumParams &P, unsigned long long &scans,
+                                       unsigned long long &probes, unsigned long long &tails, unsigned int &err) {
+    const uint32_t lane = lane_id();
+    const DevPlan *pl = P.plans + S.item_plan;
+    const uint32_t n = pl->n;
+    const uint32_t E = pl->tail_start;
+    const uint32_t L0 = S.item_depth == 0 ? 1u : S.item_depth;
+    unsigned long long cnt = 0;
+
+    if (P.mode == CSM_ENUM_MODE_EXPAND && L0 + 1 >= E) {
+        // Nothing left to expand before the counting level: pass the item through.
+        unsigned long long r = 0;
+        if (lane == 0) r = atomicAdd(&P.ctrl->out_rows, 1ull);
+        r = __shfl_sync(0xffffffffu, r, 0);
+        if (r < P.expand_cap) {
+            WorkItem *o = P.expand_out + r;
+            if (lane == 0) {
+                o->plan = S.item_plan;
+                o->depth = S.item_depth;
+                o->lo = S.item_lo;
+                o->hi = S.item_hi;
+            }
+            if (lane < CSM_MAXQV) o->f[lane] = S.f[lane];
+        } else if (lane == 0) {
+            err |= CSM_ERRBIT_OUTPUT;
+        }
+        __syncwarp();
+        return 0;
+    }
+
+    if (L0 == 1) {
+        if (lane == 0) {
+            S.lo[1] = S.item_lo;
+            S.hi[1] = S.item_hi;
+            S.nbuf[1] = 0;
+            S.pos[1] = 0;
+        }
+        __syncwarp();
+    } else {
+        enter_level(S, P, pl, L0, S.item_lo, S.item_hi);
+    }
+    uint32_t d = L0;
+    uint32_t iter = 0;
+    const uint32_t *nlf0 = bitmap(P, pl->nlf0);
+    const uint32_t *nlf1 = bitmap(P, pl->nlf1);
+
+    while (true) {
+        if (P.donate && ((++iter & 7u) == 0)) {
+            unsigned int h = 0;
+            if (lane == 0) h = *(volatile unsigned int *)&P.ctrl->hungry;
+            h = __shfl_sync(0xffffffffu, h, 0);
+            if (h > 0) try_donate(S, P, pl, L0, d);
+        }
+        if (S.pos[d] < S.nbuf[d]) {
+            // Descend into the next buffered candidate.
+            const uint32_t c = S.buf[d][S.pos[d]];
+            __syncwarp();
+            if (lane == 0) {
+                S.pos[d]++;
+                if (d == 1) {
+                    const unsigned long long key = __ldg(P.keys + c);
+                    S.f[0] = P.kl.src(key);
+                    S.f[1] = P.kl.dst(key);
+                } else {
+                    S.f[d] = c;
+                }
+            }
+            __syncwarp();
+            if (d + 1 == E) {
+                cnt += tail_count(S, P, pl, probes);
+                tails++;
+            } else {
+                d++;
+                enter_level(S, P, pl, d, 0, 0xFFFFFFFFu);
+            }
+            continue;
+        }
+        if (S.lo[d] >= S.hi[d]) {
+            if (d == L0) break;
+            d--;
+            continue;
+        }
+        // Scan the next 32 candidates of level d.
+        const uint32_t idx = S.lo[d] + lane;
+        bool ok = idx < S.hi[d];
+        uint32_t cand = 0;
+        if (d == 1) {
+            if (ok) {
+                const unsigned long long key = __ldg(P.keys + idx);
+                const uint32_t x = P.kl.src(key), y = P.kl.dst(key);
+                ok = __ldg(P.eff + idx) == P.phase && x != y && test_bit(nlf0, x) && test_bit(nlf1, y);
+                cand = idx;
+            }
+        } else {
+            const uint32_t oldm = S.oldm[d];
+            const uint32_t piv = S.piv[d];
+            if (ok) {
+                const uint32_t e = __ldg(P.g.pool + S.base[d] + idx);
+                cand = e >> 1;
+                scans++;
+                ok = !(((oldm >> piv) & 1u) && (e & 1u));
+            }
+            for (uint32_t k = 0; ok && k < d; k++) ok = S.f[k] != cand;
+            if (ok) ok = test_bit(bitmap(P, S.nlf[d]), cand);
+            const uint32_t nbn = S.nbn[d];
+            for (uint32_t k = 0; ok && k < nbn; k++) {
+                if (k == piv) continue;
+                const uint32_t e = find_entry(P.g.pool + S.poff[d][k], S.psz[d][k], cand);
+                probes++;
+                ok = e != 0xFFFFFFFFu && !(((oldm >> k) & 1u) && (e & 1u));
+            }
+        }
+        __syncwarp();
+        if (lane == 0) S.lo[d] += 32u;
+        const uint32_t mask = __ballot_sync(0xffffffffu, ok);
+        const uint32_t rank = __popc(mask & ((1u << lane) - 1u));
+        if (P.mode == CSM_ENUM_MODE_EXPAND && d == L0) {
+            // One BFS level: survivors become items of depth d + 1.
+            const uint32_t c = __popc(mask);
+            unsigned long long r = 0;
+            if (lane == 0 && c) r = atomicAdd(&P.ctrl->out_rows, (unsigned long long)c);
+            r = __shfl_sync(0xffffffffu, r, 0);
+            if (c && r + c > P.expand_cap) {
+                if (lane == 0) err |= CSM_ERRBIT_OUTPUT;
+            } else if (ok) {
+                WorkItem *o = P.expand_out + r + rank;
+                o->plan = S.item_plan;
+                o->depth = d + 1;
+                o->lo = 0;
+                o->hi = 0xFFFFFFFFu;
+                if (d == 1) {
+                    const unsigned long long key = __ldg(P.keys + cand);
+                    o->f[0] = P.kl.src(key);
+                    o->f[1] = P.kl.dst(key);
+                } else {
+                    for (uint32_t k = 0; k < d; k++) o->f[k] = S.f[k];
+                    o->f[d] = cand;
+                }
+            }
+            __syncwarp();
+        } else if (d + 1 == n) {
+            if (P.mode == CSM_ENUM_MODE_ROWS) {
+                const uint32_t c = __popc(mask);
+                unsigned long long r = 0;
+                if (lane == 0 && c) r = atomicAdd(&P.ctrl->out_rows, (unsigned long long)c);
+                r = __shfl_sync(0xffffffffu, r, 0);
+                if (c && r + c > P.row_cap) {
+                    if (lane == 0) err |= CSM_ERRBIT_OUTPUT;
+                } else if (ok) {
+                    if (d == 1) {
+                        const unsigned long long key = __ldg(P.keys + cand);
+                        uint32_t *row = P.rows + (r + rank) * CSM_ROW_WORDS;
+                        row[0] = pl->query;
+                        row[1 + pl->order[0]] = P.kl.src(key);
+                        row[1 + pl->order[1]] = P.kl.dst(key);
+                    } else {
+                        write_row(P, pl, S, d, cand, r + rank);
+                    }
+                }
+            }
+            cnt += __popc(mask);
+            __syncwarp();
+        } else {
+            if (ok) S.buf[d][rank] = cand;
+            __syncwarp();
+            if (lane == 0) {
+                S.nbuf[d] = (uint8_t)__popc(mask);
+                S.pos[d] = 0;
+            }
+            __syncwarp();
+        }
+    }
+    return cnt;
+}
+
+__global__ void __launch_bounds__(256) k_enumerate(EnumParams P) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    WarpState &S = reinterpret_cast<WarpState *>(smem)[threadIdx.x >> 5];
+    const uint32_t lane = lane_id();
+    if (P.abort_flag != nullptr && *(volatile const unsigned int *)P.abort_flag) return;
+    unsigned long long scans = 0, probes = 0, tails = 0;
+    unsigned int err = 0;
+    bool have_source = true;  // seed tickets / frontier not yet exhausted
+    while (true) {
+        int got = 0;
+        if (have_source) {
+            got = take_ticket(S, P) ? 1 : 0;
+            if (!got) have_source = false;
+        }
+        if (!got) got = claim_item(S, P, err);
+        if (got < 0) continue;  // null slot
+        if (!got) {
+            // Become idle: wait (bounded) for donated work, leave when nobody holds work.
+            if (lane == 0) {
+                atomicSub(&P.ctrl->active, 1u);
+                atomicAdd(&P.ctrl->hungry, 1u);
+            }
+            __syncwarp();
+            bool resumed = false;
+            for (uint32_t it = 0; it < P.idle_limit; it++) {
+                const int c = claim_item(S, P, err);
+                if (c != 0) {
+                    if (lane == 0) {
+                        atomicAdd(&P.ctrl->active, 1u);
+                        atomicSub(&P.ctrl->hungry, 1u);
+                    }
+                    __syncwarp();
+                    if (c > 0) resumed = true;
+                    else {
+                        if (lane == 0) {
+                            atomicSub(&P.ctrl->active, 1u);
+                            atomicAdd(&P.ctrl->hungry, 1u);
+                        }
+                        __syncwarp();
+                        continue;
+                    }
+                    break;
+                }
+                unsigned int act = 0, qr = 0, qw = 0;
+                if (lane == 0) {
+                    act = *(volatile unsigned int *)&P.ctrl->active;
+                    qr = *(volatile unsigned int *)&P.ctrl->q_read;
+                    qw = *(volatile unsigned int *)&P.ctrl->q_write;
+                }
+                act = __shfl_sync(0xffffffffu, act, 0);
+                qr = __shfl_sync(0xffffffffu, qr, 0);
+                qw = __shfl_sync(0xffffffffu, qw, 0);
+                if (qw > P.qcap) qw = P.qcap;
+                if (act == 0 && qr >= qw) break;
+                __nanosleep(512);
+            }
+            if (!resumed) {
+                if (lane == 0) atomicSub(&P.ctrl->hungry, 1u);
+                break;
+            }
+        }
+        const unsigned long long c = run_item(S, P, scans, probes, tails, err);
+        if (lane == 0 && c) atomicAdd(P.counts + S.item_plan, c);
+        __syncwarp();
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        scans += __shfl_xor_sync(0xffffffffu, scans, o);
+        probes += __shfl_xor_sync(0xffffffffu, probes, o);
+    }
+    if (lane == 0) {
+        if (scans) atomicAdd(&P.ctrl->scan_entries, scans);
+        if (probes) atomicAdd(&P.ctrl->probes, probes);
+        if (tails) atomicAdd(&P.ctrl->tail_lists, tails);
+        if (err) atomicOr(&P.ctrl->error, err);
+    }
+}
+
+// Per plan: the key range of its seed relation, and the number of 32-key seed chunks.
+__global__ void k_seed_ranges(const DevPlan *plans, uint32_t nplans, const unsigned long long *keys, uint32_t m,
+                              KeyLayout kl, uint32_t *seed_lo, uint32_t *chunks) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= nplans) return;
+    const uint32_t rel = plans[p].seed_rel;
+    // [lo, hi) = keys whose relation field equals rel.
+    uint32_t lo = 0, hi = m;
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (kl.rel(keys[mid]) < rel) lo = mid + 1;
+        else hi = mid;
+    }
+    uint32_t a = lo;
+    lo = a;
+    hi = m;
+    while (lo < hi) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (kl.rel(keys[mid]) <= rel) lo = mid + 1;
+        else hi = mid;
+    }
+    seed_lo[p] = a;
+    seed_lo[nplans + p] = lo;
+    chunks[p] = (lo - a + 31u) / 32u;
+}
+
+// Exclusive prefix of chunk counts (one block; plans are few).
+__global__ void k_ticket_prefix(const uint32_t *chunks, uint32_t nplans, uint32_t *prefix, EnumControl *ctrl) {
+    __shared__ uint32_t part[1024];
+    const uint32_t t = threadIdx.x;
+    const uint32_t per = (nplans + blockDim.x - 1) / blockDim.x;
+    uint32_t s = 0;
+    for (uint32_t i = t * per; i < (t + 1) * per && i < nplans; i++) s += chunks[i];
+    part[t] = s;
+    __syncthreads();
+    if (t == 0) {
+        uint32_t acc = 0;
+        for (uint32_t i = 0; i < blockDim.x; i++) {
+            uint32_t v = part[i];
+            part[i] = acc;
+            acc += v;
+        }
+        ctrl->nticket = acc;
+        prefix[nplans] = acc;
+    }
+    __syncthreads();
+    uint32_t acc = part[t];
+    for (uint32_t i = t * per; i < (t + 1) * per && i < nplans; i++) {
+        prefix[i] = acc;
+        acc += chunks[i];
+    }
+}
+
+__global__ void k_ctrl_reset(EnumControl *ctrl, uint32_t active, uint32_t epoch, unsigned long long nticket) {
+    EnumControl c;
+    memset(&c, 0, sizeof(c));
+    c.active = active;
+    c.epoch = epoch;
+    c.nticket = nticket;
+    *ctrl = c;
+}
+
+// Upper bound of the next BFS level: sum over items of their smallest candidate list.
+__global__ void k_expand_bound(EnumParams P, const WorkItem *items, const unsigned long long *nitems) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const unsigned long long nw = (unsigned long long)gridDim.x * (blockDim.x >> 5);
+    const unsigned long long n = *nitems;
+    unsigned long long acc = 0;
+    for (unsigned long long i = (blockIdx.x * (blockDim.x >> 5)) + (threadIdx.x >> 5); i < n; i += nw) {
+        const WorkItem *it = items + i;
+        const DevPlan *pl = P.plans + it->plan;
+        const uint32_t d = it->depth;
+        if (d + 1 >= pl->tail_start) {
+            if (lane == 0) acc += 1;  // passes through unchanged
+            continue;
+        }
+        const DevLevel *lv = &pl->lv[d];
+        uint32_t sz = 0xFFFFFFFFu;
+        if (lane < lv->nbn) {
+            const uint2 ms = P.g.meta[(size_t)lv->bn_rel[lane] * P.g.V + it->f[lv->bn_depth[lane]]];
+            sz = ms.y;
+        }
+        for (int o = 16; o > 0; o >>= 1) sz = min(sz, __shfl_xor_sync(0xffffffffu, sz, o));
+        if (lane == 0) acc += sz;
+    }
+    if (lane == 0 && acc) atomicAdd(&P.ctrl->expand_bound, acc);
+}
+
+}  // namespace
+
+size_t enum_smem_bytes(int warps_per_block) { return sizeof(WarpState) * (size_t)warps_per_block; }
+
+void launch_enumerate(const EnumParams &p, int blocks, int warps_per_block, cudaStream_t s) {
+    const size_t smem = enum_smem_bytes(warps_per_block);
+    cudaFuncSetAttribute(k_enumerate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_enumerate<<<blocks, warps_per_block * 32, smem, s>>>(p);
+}
+
+void launch_seed_tickets(const DevPlan *plans, uint32_t nplans, const unsigned long long *keys, uint32_t m,
+                         KeyLayout kl, uint32_t *seed_lo, uint32_t *ticket_prefix, EnumControl *ctrl,
+                         cudaStream_t s) {
+    // seed_lo holds three arrays of nplans: first key, end key, chunk count.
+    uint32_t *chunks = seed_lo + 2 * nplans;
+    k_seed_ranges<<<(nplans + 127) / 128, 128, 0, s>>>(plans, nplans, keys, m, kl, seed_lo, chunks);
+    k_ticket_prefix<<<1, 1024, 0, s>>>(chunks, nplans, ticket_prefix, ctrl);
+}
+
+void launch_ctrl_reset(EnumControl *ctrl, uint32_t active, uint32_t epoch, unsigned long long nticket,
+                       cudaStream_t s) {
+    k_ctrl_reset<<<1, 1, 0, s>>>(ctrl, active, epoch, nticket);
+}
+
+void launch_expand_bound(const EnumParams &p, const WorkItem *items, const unsigned long long *nitems,
+                         cudaStream_t s) {
+    k_expand_bound<<<296, 256, 0, s>>>(p, items, nitems);
+}
+
+}  // namespace csm
