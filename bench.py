@@ -1,0 +1,364 @@
+"""Benchmark of the batch-update incremental matching path.
+
+Workload (default): the Amazon-shaped configuration — Chung-Lu graph, 400k vertices, 2.4M
+edges, exponent 2.1, 6 Zipf(1.0) vertex labels; ten 6-vertex standing queries (5 dense, 5
+trees) sampled from the graph; 240k updates (90% insertions of held-out edges, 10% deletions)
+in batches of 65,536.  Seeded synthetic data stands in for the datasets the reference's
+experiments download.
+
+A step applies one update batch and counts its incremental matches (positive and negative)
+for all standing queries.  The stream of four batches is followed by its inverse (each batch
+undone, last first), so any number of steps replays a well-defined state sequence.
+
+Metric: incremental matches per second = sum over steps of (positive + negative) / time.
+  value — device-resident update arrays (csm_apply_batch_device), CUDA-event time.
+  e2e   — host update arrays through csm_apply_batch: the host->device copy of each batch and the
+          readback of its counts are inside the timed region.
+Under torchrun every rank runs an independent replica (weak scaling) and the time is the
+maximum over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "gcsm-bu_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import numpy as np  # noqa: E402
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2")
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--nqueries", type=int, default=None)
+    ap.add_argument("--strategy", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-queries", type=int, default=10)
+    return ap.parse_args()
+
+
+def inverse(b):
+    from csm import Batch
+    dl = b.is_delete if b.is_delete is not None else np.zeros(len(b.src), dtype=np.uint8)
+    return Batch(b.src, b.dst, b.elabels, (1 - dl).astype(np.uint8))
+
+
+def step_batches(w, count):
+    seq = list(w.batches) + [inverse(b) for b in reversed(w.batches)]
+    return [seq[i % len(seq)] for i in range(count)]
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi while the timed region runs."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._th = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self._p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                        "--format=csv,noheader,nounits", "-lms", "100"],
+                                       stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._th = threading.Thread(target=self._read, daemon=True)
+            self._th.start()
+        except FileNotFoundError:
+            self._p = None
+        return self
+
+    def _read(self):
+        for line in self._p.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 7:
+                self.samples.append(parts)
+
+    def __exit__(self, *exc):
+        if self._p is not None:
+            self._p.terminate()
+            try:
+                self._p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self._p.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per enumeration launch from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "enumerate_traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return None
+
+
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        if backend == "nccl":
+            import torch
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world, device=None):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_baseline(w, args, max_seconds=20.0):
+    """The oracle on the host cores over a bounded sample of the workload."""
+    from oracle import Oracle
+    threads = os.cpu_count() or 1
+    qs = w.queries[: args.cpu_sample_queries]
+    t_total, matches, batches_done = 0.0, 0, 0
+    oracles = [Oracle(q, w.data) for q in qs]
+    for b in w.batches:
+        for o in oracles:
+            t0 = time.perf_counter()
+            r = o.apply(b, threads=threads)
+            t_total += time.perf_counter() - t0
+            matches += r["pos"] + r["neg"]
+        batches_done += 1
+        if t_total > max_seconds:
+            break
+    for o in oracles:
+        o.close()
+    return {"value": matches / t_total if t_total else None, "unit": "matches/s", "cores": threads, "kind": "port",
+            "sample": f"first {batches_done} batch(es) of the stream x {len(qs)} queries, "
+                      f"{matches} matches in {t_total:.2f} s"}, matches, t_total
+
+
+def run_reference(args, w, world, rank):
+    """CPU implementation of the path (the oracle port) on all host threads, same steps."""
+    if rank != 0:
+        return
+    from oracle import Oracle
+    threads = os.cpu_count() or 1
+    oracles = [Oracle(q, w.data) for q in w.queries]
+    seq = step_batches(w, args.warmup + args.steps)
+    # Bound the run: each step is capped to the queries that fit the time budget.
+    for b in seq[: args.warmup]:
+        for o in oracles:
+            o.apply(b, threads=threads)
+    t_total, matches, upd = 0.0, 0, 0
+    lat = []
+    for b in seq[args.warmup:]:
+        t0 = time.perf_counter()
+        for o in oracles:
+            r = o.apply(b, threads=threads)
+            matches += r["pos"] + r["neg"]
+        dt = time.perf_counter() - t0
+        lat.append(dt)
+        t_total += dt
+        upd += len(b.src)
+    value = matches / t_total
+    out = {
+        "metric": "incremental matches/sec", "value": value, "unit": "matches/s", "impl": "reference",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": f"{w.name}: Chung-Lu {len(w.data.vlabels)} vertices, "
+                               f"{len(w.data.src)} initial edges, {len(w.queries)} standing queries, "
+                               f"batches of {w.batch_size} updates", "batch_size": w.batch_size,
+                   "queries": len(w.queries), "parallelism": "replicas"},
+        "update_edges_per_s": upd / t_total,
+        "p50_batch_ms": 1e3 * float(np.percentile(lat, 50)), "p99_batch_ms": 1e3 * float(np.percentile(lat, 99)),
+        "cpu_baseline": {"value": value, "unit": "matches/s", "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} steps x {len(w.queries)} queries (full steps)"},
+        "e2e": {"value": value, "unit": "matches/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+
+
+def run_ours(args, w, world, rank, local):
+    import torch
+
+    import csm
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    eng = csm.Engine(device=local, algorithm=0, search_strategy=args.strategy, max_batch=w.batch_size)
+    for q in w.queries:
+        eng.load_query(q)
+    eng.load_graph(w.data)
+    stream = torch.cuda.current_stream(dev)
+    cache = {}
+
+    def on_device(b):
+        key = id(b)
+        if key not in cache:
+            dl = b.is_delete if b.is_delete is not None else np.zeros(len(b.src), dtype=np.uint8)
+            cache[key] = tuple(torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+                               for a in (b.src.astype(np.int32), b.dst.astype(np.int32),
+                                         b.elabels.astype(np.int32), dl.astype(np.uint8)))
+        return cache[key]
+
+    def apply_dev(b):
+        s, d, l, dl = on_device(b)
+        return eng.apply_device(len(b.src), s.data_ptr(), d.data_ptr(), l.data_ptr(), dl.data_ptr(),
+                                stream.cuda_stream)
+
+    seq = step_batches(w, args.warmup + 2 * args.steps)
+    warm, timed, timed_e2e = seq[: args.warmup], seq[args.warmup: args.warmup + args.steps], seq[args.warmup + args.steps:]
+    for b in warm + timed + timed_e2e:
+        on_device(b)
+    for b in warm:
+        apply_dev(b)
+    torch.cuda.synchronize(dev)
+    eng.reset_stats()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    matches, upd, lat = 0, 0, []
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for b in timed:
+            res = apply_dev(b)
+            matches += sum(r.positive + r.negative for r in res)
+            upd += int(res[0].inserted + res[0].deleted)
+            lat.append(res[0].latency_ns / 1e6)
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+    barrier(world)
+    t = ev0.elapsed_time(ev1) / 1e3
+    tmax = max_over_ranks(t, world, dev)
+    st = eng.stats()
+
+    # End to end: host (pinned) update arrays through csm_apply_batch, next steps of the cycle.
+    pinned = {}
+    for b in timed_e2e:
+        if id(b) not in pinned:
+            arrs = []
+            for a, dt in ((b.src, torch.int32), (b.dst, torch.int32), (b.elabels, torch.int32)):
+                h = torch.empty(len(a), dtype=dt, pin_memory=True)
+                h.numpy()[:] = a.view(np.int32)
+                arrs.append(h)
+            dl = b.is_delete if b.is_delete is not None else np.zeros(len(b.src), dtype=np.uint8)
+            h = torch.empty(len(dl), dtype=torch.uint8, pin_memory=True)
+            h.numpy()[:] = dl
+            arrs.append(h)
+            pinned[id(b)] = arrs
+    matches_e2e, h2d = 0, 0
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for b in timed_e2e:
+        s, d, l, dl = pinned[id(b)]
+        res = eng.apply(csm.Batch(s.numpy().view(np.uint32), d.numpy().view(np.uint32), l.numpy().view(np.uint32),
+                                  dl.numpy()))
+        matches_e2e += sum(r.positive + r.negative for r in res)
+        h2d += 13 * len(b.src)
+    t_e2e = time.perf_counter() - t0
+    t_e2e_max = max_over_ranks(t_e2e, world, dev)
+    pool_mb = st.pool_capacity * 4 / 2 ** 20
+    eng.close()
+    if rank != 0:
+        return
+    peak, peak_kind = measured_peaks()
+    alg_bytes = 4.0 * (st.enum_scan_entries + st.enum_probes + st.enum_tail_lists)
+    enum_s = st.enum_ns / 1e9
+    launches = max(1, st.enum_launches)
+    achieved = alg_bytes / enum_s / 1e9 if enum_s > 0 else 0.0
+    traffic = profile_traffic()
+    clocks = clk.summary()
+    out = {
+        "metric": "incremental matches/sec", "value": world * matches / tmax, "unit": "matches/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tmax / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": {"workload": f"{w.name}: Chung-Lu {len(w.data.vlabels)} vertices, {len(w.data.src)} initial edges,"
+                               f" {len(w.queries)} standing queries, batches of {w.batch_size} updates"
+                               " (stream then its inverse)",
+                   "batch_size": w.batch_size, "queries": len(w.queries), "search_strategy": args.strategy,
+                   "parallelism": f"replicas x{world}",
+                   "l2": f"inputs larger than L2 (adjacency pool {pool_mb:.0f} MiB, 126 MB L2)"},
+        "update_edges_per_s": world * upd / tmax,
+        "p50_batch_ms": float(np.percentile(lat, 50)), "p99_batch_ms": float(np.percentile(lat, 99)),
+        "matches_per_step": matches / args.steps,
+        "e2e": {"value": world * matches_e2e / t_e2e_max, "unit": "matches/s",
+                "h2d_bytes_per_step": h2d // max(1, len(timed_e2e)),
+                "d2h_bytes_per_step": 64 * len(w.queries)},
+        "gpu_launches": int(st.kernel_launches),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": f"{peak_kind} hbm_gbs",
+                     "kernel": "k_enumerate",
+                     "algorithmic_bytes_per_launch": alg_bytes / launches,
+                     "avg_launch_ms": 1e3 * enum_s / launches,
+                     "traffic": traffic.get("dram_bytes_per_launch") if traffic else None},
+        "phase_ms": {"enumerate": 1e3 * enum_s / args.steps, "apply": st.apply_ns / 1e6 / args.steps},
+        "clocks": clocks,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        cb, _, _ = cpu_baseline(w, args)
+        out["cpu_baseline"] = cb
+    print(json.dumps(out))
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_init(args)
+    from csm import gen
+    cfg = gen.scaled(args.config, args.scale) if args.scale != 1.0 else None
+    w = gen.make_workload(args.config, cfg, nqueries=args.nqueries)
+    if args.impl == "reference":
+        run_reference(args, w, world, rank)
+    else:
+        run_ours(args, w, world, rank, local)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -128,7 +128,25 @@ def sample_query(adj: Adjacency, vlab: np.ndarray, k: int, kind: str, rng: np.ra
                               np.array([e[0] for e in edges], dtype=np.uint32),
                               np.array([e[1] for e in edges], dtype=np.uint32),
                               np.array([e[2] for e in edges], dtype=np.uint32))
-        # dense
+        # dense: a random walk until k distinct vertices, induced subgraph; half of the tries
+        # grow greedily instead (most edges into the set), which finds dense sets when walks fail.
+        if rng.random() < 0.5:
+            vs, cur, steps = [v0], v0, 0
+            while len(vs) < k and steps < 50 * k:
+                nb = adj.nbrs(cur)
+                cur = int(nb[rng.integers(len(nb))])
+                if cur not in vs:
+                    vs.append(cur)
+                steps += 1
+            if len(vs) < k:
+                continue
+            q = _induced(adj, vs, vlab)
+            m = len(q.src)
+            if 2 * m >= 3 * k:
+                return q
+            if m > best_m:
+                best, best_m = q, m
+            continue
         vs = [v0, int(rng.choice(adj.nbrs(v0)))]
         while len(vs) < k:
             cand = {}

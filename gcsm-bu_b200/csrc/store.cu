@@ -377,7 +377,7 @@ __global__ void k_copy_lists(size_t n, const uint2 *meta, const unsigned long lo
     const size_t nw = (size_t)gridDim.x * (blockDim.x >> 5);
     for (size_t i = blockIdx.x * (size_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += nw) {
         const uint2 ms = meta[i];
-        for (uint32_t j = lane; j < ms.y; j += 32) dst[newoff[i] + j] = src[ms.x + j] & ~1u;
+        for (uint32_t j = lane; j < ms.y; j += 32) dst[newoff[i] + j] = src[ms.x + j];
     }
 }
 

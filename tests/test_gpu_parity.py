@@ -1,0 +1,147 @@
+"""GPU parity: the CUDA engine (through the C ABI) against the CPU oracle, batch by batch.
+
+Counts are integers and must be bit-exact: positive and negative incremental matches per
+batch and per query, the per-query-edge split, and (with materialisation) the sorted rows.
+"""
+import numpy as np
+import pytest
+
+import csm
+from csm import Batch, DataGraph, QueryGraph, gen
+from oracle import Oracle
+from helpers import clique, cycle, path, random_graph, small_workload, star
+
+pytestmark = pytest.mark.gpu
+
+
+def check_stream(w, queries=None, batches=None, rows=False, **cfg):
+    queries = w.queries if queries is None else queries
+    batches = w.batches if batches is None else batches
+    if rows:
+        cfg.setdefault("materialize_rows", 1 << 22)
+    eng = csm.Engine(**cfg)
+    for q in queries:
+        eng.load_query(q)
+    eng.load_graph(w.data)
+    oracles = [Oracle(q, w.data) for q in queries]
+    totals = [0, 0]
+    for bi, b in enumerate(batches):
+        res = eng.apply(b)
+        for qi, o in enumerate(oracles):
+            r = o.apply(b, rows=rows)
+            got = (res[qi].positive, res[qi].negative)
+            assert got == (r["pos"], r["neg"]), f"batch {bi} query {qi}: engine {got} oracle {(r['pos'], r['neg'])}"
+            pos, neg = eng.edge_counts(qi)
+            assert pos == r["per_qe_pos"] and neg == r["per_qe_neg"], f"batch {bi} query {qi} per-edge split"
+            if rows:
+                assert np.array_equal(eng.embeddings(qi, 1), o.rows(1)), f"batch {bi} query {qi} positive rows"
+                assert np.array_equal(eng.embeddings(qi, -1), o.rows(-1)), f"batch {bi} query {qi} negative rows"
+            totals[0] += r["pos"]
+            totals[1] += r["neg"]
+    eng.close()
+    return totals
+
+
+@pytest.fixture(scope="module")
+def c1():
+    return small_workload("c1")
+
+
+@pytest.mark.parametrize("strategy", [0, 1, 2, 3])
+def test_c1_search_strategies(c1, strategy):
+    tot = check_stream(c1, algorithm=0, search_strategy=strategy)
+    assert tot[0] > 0
+
+
+@pytest.mark.parametrize("algorithm", [1, 2, 4, 5])
+def test_c1_algorithm_presets(c1, algorithm):
+    check_stream(c1, algorithm=algorithm)
+
+
+@pytest.mark.parametrize("order", [0, 1, 2, 3])
+def test_c1_matching_orders_no_cartesian(c1, order):
+    check_stream(c1, algorithm=0, matching_order=order, cartesian_product=0)
+
+
+def test_c1_rows(c1):
+    w = small_workload("c1", scale=0.3)
+    check_stream(w, rows=True)
+
+
+def test_amazon_shaped_small_with_deletions():
+    w = small_workload("c2", scale=0.005, batch=700, nqueries=6)
+    tot = check_stream(w, search_strategy=2)
+    assert tot[1] > 0
+
+
+def test_amazon_shaped_small_dfs_with_stealing():
+    w = small_workload("c2", scale=0.005, batch=1500, nqueries=6)
+    check_stream(w, search_strategy=0)
+
+
+def test_rows_with_deletions():
+    w = small_workload("c2", scale=0.002, batch=300, nqueries=3)
+    check_stream(w, rows=True)
+
+
+def test_multi_query_mixed_sizes():
+    w = small_workload("c4", scale=0.002, batch=500, nqueries=6)
+    check_stream(w)
+
+
+def test_heavy_vertex_dense8():
+    w = small_workload("c3", scale=0.0005, batch=2000, nqueries=2)
+    check_stream(w)
+
+
+def test_edge_cases_in_batches():
+    rng = np.random.default_rng(7)
+    vl, s, d, el = random_graph(60, 300, 2, rng)
+    data = DataGraph(vl, s, d, el)
+    w = gen.Workload("edge", data, [], [cycle(4, [0, 1, 0, 1]), clique(3), star(3), path(4)], 0)
+    n = len(vl)
+    batches = [
+        Batch(np.zeros(0, np.uint32), np.zeros(0, np.uint32), np.zeros(0, np.uint32)),         # empty
+        Batch(s[:5], d[:5], el[:5]),                                                           # existing edges
+        Batch(np.array([3, 3, 5, 5], np.uint32), np.array([3, 9, 9, 3], np.uint32),
+              np.zeros(4, np.uint32)),                                                         # self-loop + dups
+        Batch(np.array([1, 2, n + 5], np.uint32), np.array([40, 41, 2], np.uint32),
+              np.zeros(3, np.uint32), np.array([1, 1, 0], np.uint8)),                          # absent deletes, out of range
+        Batch(s[10:20], d[10:20], el[10:20], np.ones(10, np.uint8)),                           # deletions
+        Batch(np.concatenate([s[10:15], s[30:35]]), np.concatenate([d[10:15], d[30:35]]),
+              np.concatenate([el[10:15], el[30:35]]),
+              np.array([0] * 5 + [1] * 5, np.uint8)),                                           # re-insert + delete
+        Batch(np.array([7, 7], np.uint32), np.array([8, 8], np.uint32), np.zeros(2, np.uint32),
+              np.array([1, 0], np.uint8)),                                                      # insert wins
+    ]
+    for strategy in (0, 2):
+        check_stream(w, batches=batches, search_strategy=strategy)
+
+
+@pytest.mark.parametrize("bs", [1, 13])
+def test_tiny_batches(bs):
+    w = small_workload("c1", scale=0.05)
+    xs = np.concatenate([b.src for b in w.batches])[:300]
+    ys = np.concatenate([b.dst for b in w.batches])[:300]
+    ls = np.concatenate([b.elabels for b in w.batches])[:300]
+    batches = [Batch(xs[i:i + bs], ys[i:i + bs], ls[i:i + bs]) for i in range(0, len(xs), bs)][:60]
+    check_stream(w, batches=batches)
+
+
+def test_pool_regrowth_keeps_counts():
+    w = small_workload("c2", scale=0.005, batch=2000, nqueries=3)
+    # A pool barely larger than the initial layout forces relocation, overflow and regrowth.
+    eng = csm.Engine()
+    for q in w.queries:
+        eng.load_query(q)
+    eng.load_graph(w.data)
+    used = eng.stats().pool_used
+    eng.close()
+    tot = check_stream(w, pool_entries=int(used * 1.05) + 64)
+    assert tot[0] > 0
+
+
+def test_launch_shapes_and_steal_chunk():
+    w = small_workload("c2", scale=0.003, batch=3000, nqueries=4)
+    for bps, wpb, sc in ((1, 1, 32), (2, 4, 128), (8, 8, 64)):
+        check_stream(w, blocks_per_sm=bps, warps_per_block=wpb, steal_chunk=sc, search_strategy=0)

@@ -1,0 +1,60 @@
+"""CPU tests of the C-ABI boundary: the library loads, exports every declared symbol, and fails
+loudly (no fallback) when no GPU is present."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+import csm
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def ensure_built():
+    if not os.path.exists(csm.LIB_PATH) or not os.path.exists(csm.CSMG_PATH):
+        subprocess.run(["make", "-s", "-j8", "-C", os.path.join(ROOT, "gcsm-bu_b200")], check=True)
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "csm.h")).read()
+    return sorted(set(re.findall(r"\b(csm_[a-z_]+)\s*\(", text)))
+
+
+def test_header_matches_python_binding():
+    assert declared_symbols() == sorted(csm.EXPORTED)
+
+
+def test_library_exports_every_declared_symbol():
+    ensure_built()
+    lib = ctypes.CDLL(csm.LIB_PATH)
+    for name in declared_symbols():
+        assert hasattr(lib, name), name
+    out = subprocess.run(["nm", "-D", "--defined-only", csm.LIB_PATH], capture_output=True, text=True).stdout
+    exported = sorted(set(re.findall(r" T (csm_\w+)", out)))
+    assert exported == declared_symbols()
+
+
+def test_version_and_default_config():
+    ensure_built()
+    assert "sm_100a" in csm.version()
+    cfg = csm.default_config()
+    assert cfg.algorithm == 0 and cfg.matching_order == 2 and cfg.search_strategy == 2
+    assert cfg.local_index == 1 and cfg.cartesian_product == 1
+
+
+def test_create_fails_loudly_without_gpu():
+    ensure_built()
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(csm.CsmError) as ei:
+        csm.Engine()
+    assert ei.value.code in (-8, -2)
+
+
+def test_struct_layouts():
+    assert ctypes.sizeof(csm.CsmConfig) == 4 * 8 + 8 * 4 + 4 * 8
+    assert ctypes.sizeof(csm.CsmBatchResult) == 64
+    assert ctypes.sizeof(csm.CsmStats) == 16 * 8
