@@ -31,6 +31,7 @@
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
+#include <time.h>
 
 #define MAXQV 16
 #define MAXQE 42
@@ -116,6 +117,13 @@ static int adj_remove(Adj *A, uint32_t v, uint32_t l) {
     return 1;
 }
 
+static int nbr_sort_cmp(const void *pa, const void *pb) {
+    const Nbr *a = (const Nbr *)pa, *b = (const Nbr *)pb;
+    if (a->v != b->v) return a->v < b->v ? -1 : 1;
+    if (a->l != b->l) return a->l < b->l ? -1 : 1;
+    return 0;
+}
+
 static int ekey_cmp(const void *pa, const void *pb) {
     const EKey *a = (const EKey *)pa, *b = (const EKey *)pb;
     if (a->x != b->x) return a->x < b->x ? -1 : 1;
@@ -177,12 +185,39 @@ void *oracle_create(uint32_t qn, const uint32_t *qvl, uint32_t qm, const uint32_
     o->adj = (Adj *)calloc(nv ? nv : 1, sizeof(Adj));
     if (!o->vlab || !o->adj) return NULL;
     memcpy(o->vlab, vl, sizeof(uint32_t) * nv);
+    /* Bulk build: count, fill, then sort and deduplicate each list. */
+    uint32_t *deg = (uint32_t *)calloc(nv ? nv : 1, sizeof(uint32_t));
+    if (!deg) return NULL;
     for (uint64_t e = 0; e < ne; e++) {
         uint32_t x = es[e], y = ed[e];
         if (x >= nv || y >= nv || x == y) continue;
-        adj_insert(&o->adj[x], y, el[e]);
-        adj_insert(&o->adj[y], x, el[e]);
+        deg[x]++;
+        deg[y]++;
     }
+    for (uint32_t v = 0; v < nv; v++) {
+        o->adj[v].cap = deg[v] ? deg[v] : 0;
+        o->adj[v].a = deg[v] ? (Nbr *)malloc(sizeof(Nbr) * deg[v]) : NULL;
+        if (deg[v] && !o->adj[v].a) return NULL;
+    }
+    for (uint64_t e = 0; e < ne; e++) {
+        uint32_t x = es[e], y = ed[e];
+        if (x >= nv || y >= nv || x == y) continue;
+        Adj *A = &o->adj[x], *B = &o->adj[y];
+        A->a[A->n].v = y;
+        A->a[A->n++].l = el[e];
+        B->a[B->n].v = x;
+        B->a[B->n++].l = el[e];
+    }
+    for (uint32_t v = 0; v < nv; v++) {
+        Adj *A = &o->adj[v];
+        if (A->n < 2) continue;
+        qsort(A->a, A->n, sizeof(Nbr), nbr_sort_cmp);
+        uint32_t w = 1;
+        for (uint32_t i = 1; i < A->n; i++)
+            if (A->a[i].v != A->a[w - 1].v || A->a[i].l != A->a[w - 1].l) A->a[w++] = A->a[i];
+        A->n = w;
+    }
+    free(deg);
     return o;
 }
 
@@ -236,8 +271,26 @@ typedef struct {
     Order ord[MAXQE];
     atomic_ulong next;
     uint64_t nitems; /* qm * nnew * 2 */
+    uint64_t stride; /* items are visited in the order (k * stride) mod nitems */
     int want_rows;
+    double deadline; /* CLOCK_MONOTONIC seconds; 0 = none */
+    atomic_ulong done;
 } Job;
+
+static double now_s(void) {
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return ts.tv_sec + 1e-9 * ts.tv_nsec;
+}
+
+static uint64_t gcd64(uint64_t a, uint64_t b) {
+    while (b) {
+        uint64_t t = a % b;
+        a = b;
+        b = t;
+    }
+    return a;
+}
 
 typedef struct {
     Job *job;
@@ -246,6 +299,7 @@ typedef struct {
     uint64_t nrows, cap;
     uint64_t scan, probe;
     int oom;
+    int stop; /* deadline passed inside an item */
 } Worker;
 
 static void emit_row(Worker *w, const Order *ord, const uint32_t *f) {
@@ -273,20 +327,25 @@ static void extend(Worker *w, uint32_t qe, const Order *ord, uint32_t d, uint32_
         return;
     }
     const uint32_t u = ord->order[d];
-    const uint32_t p = ord->bn[d][0];
+    /* Scan the smallest backward-neighbour list, probe the others. */
+    uint32_t pk = 0;
+    for (uint32_t b = 1; b < ord->nbn[d]; b++)
+        if (o->adj[f[ord->bn[d][b]]].n < o->adj[f[ord->bn[d][pk]]].n) pk = b;
+    const uint32_t p = ord->bn[d][pk];
     const uint32_t pu = ord->order[p];
     const uint32_t l0 = o->qel[pu][u];
     const int old0 = o->qidx[pu][u] > (int)qe;
     const Adj *A = &o->adj[f[p]];
-    for (uint32_t i = adj_lb(A, 0, 0); i < A->n; i++) {
+    for (uint32_t i = 0; i < A->n && !w->stop; i++) {
         const uint32_t c = A->a[i].v;
-        w->scan++;
+        if ((++w->scan & 4095u) == 0 && w->job->deadline > 0 && now_s() > w->job->deadline) w->stop = 1;
         if (A->a[i].l != l0 || o->vlab[c] != o->qlab[u]) continue;
         int ok = 1;
         for (uint32_t k = 0; k < d && ok; k++) ok = f[k] != c;
         if (!ok) continue;
         if (old0 && in_set(w->job->newset, w->job->nnew, f[p], c, l0)) continue;
-        for (uint32_t b = 1; b < ord->nbn[d] && ok; b++) {
+        for (uint32_t b = 0; b < ord->nbn[d] && ok; b++) {
+            if (b == pk) continue;
             const uint32_t bd = ord->bn[d][b];
             const uint32_t bu = ord->order[bd];
             const uint32_t lb = o->qel[bu][u];
@@ -306,8 +365,11 @@ static void *worker_main(void *arg) {
     const Oracle *o = job->o;
     uint32_t f[MAXQV];
     for (;;) {
-        uint64_t it = atomic_fetch_add(&job->next, 1);
-        if (it >= job->nitems) break;
+        uint64_t k = atomic_fetch_add(&job->next, 1);
+        if (k >= job->nitems || w->stop) break;
+        if (job->deadline > 0 && now_s() > job->deadline) break;
+        atomic_fetch_add(&job->done, 1);
+        const uint64_t it = (k * job->stride) % job->nitems;
         const uint32_t qe = (uint32_t)(it / (job->nnew * 2));
         const uint64_t rem = it % (job->nnew * 2);
         const EKey *e = &job->newset[rem / 2];
@@ -333,7 +395,7 @@ static int row_cmp(const void *a, const void *b) {
 
 /* Counts embeddings of the current graph that use >= 1 edge of `newset` (sorted, unique). */
 static int delta(Oracle *o, const EKey *newset, uint64_t nnew, int nthreads, int want_rows, uint64_t *per_qe,
-                 uint32_t **rows_out, uint64_t *nrows_out) {
+                 uint32_t **rows_out, uint64_t *nrows_out, double deadline, uint64_t *items) {
     Job job;
     memset(&job, 0, sizeof job);
     job.o = o;
@@ -341,7 +403,16 @@ static int delta(Oracle *o, const EKey *newset, uint64_t nnew, int nthreads, int
     job.nnew = nnew;
     job.want_rows = want_rows;
     job.nitems = (uint64_t)o->qm * nnew * 2;
+    job.deadline = deadline;
+    job.stride = 1;
+    if (deadline > 0 && job.nitems > 1) {
+        /* Sampling: visit items in a scattered order so a deadline cuts an unbiased subset. */
+        uint64_t st = 2654435761ull % job.nitems;
+        while (st < 2 || gcd64(st, job.nitems) != 1) st++;
+        job.stride = st;
+    }
     atomic_init(&job.next, 0);
+    atomic_init(&job.done, 0);
     for (uint32_t i = 0; i < o->qm; i++) bfs_order(o, o->qe_a[i], o->qe_b[i], &job.ord[i]);
     if (nthreads < 1) nthreads = 1;
     if (nthreads > 256) nthreads = 256;
@@ -379,6 +450,7 @@ static int delta(Oracle *o, const EKey *newset, uint64_t nnew, int nthreads, int
         *rows_out = all;
         *nrows_out = total_rows;
     }
+    if (items) *items += atomic_load(&job.done);
     for (int t = 0; t < nthreads; t++) free(ws[t].rows);
     free(ws);
     free(th);
@@ -389,9 +461,11 @@ static int delta(Oracle *o, const EKey *newset, uint64_t nnew, int nthreads, int
  * Applies one batch; fills out[0] = positive, out[1] = negative and per_qe[0..qm) positive,
  * per_qe[qm..2qm) negative counts per query edge (qe_list_ order).  Returns 0 on success.
  */
-int oracle_apply(void *h, uint64_t nb, const uint32_t *bs, const uint32_t *bd, const uint32_t *bl, const uint8_t *bdel,
-                 int nthreads, int want_rows, uint64_t *out, uint64_t *per_qe) {
+static int apply_impl(void *h, uint64_t nb, const uint32_t *bs, const uint32_t *bd, const uint32_t *bl,
+                      const uint8_t *bdel, int nthreads, int want_rows, uint64_t *out, uint64_t *per_qe,
+                      double max_seconds, uint64_t *items) {
     Oracle *o = (Oracle *)h;
+    const double deadline = max_seconds > 0 ? now_s() + max_seconds : 0.0;
     if (!o) return -1;
     /* Net effect of the batch: an insertion wins over a deletion of the same edge. */
     EKey *ins = (EKey *)malloc(sizeof(EKey) * (nb + 1)), *del = (EKey *)malloc(sizeof(EKey) * (nb + 1));
@@ -432,7 +506,7 @@ int oracle_apply(void *h, uint64_t nb, const uint32_t *bs, const uint32_t *bd, c
     o->b_scan = o->b_probe = 0;
     int rc = 0;
     /* Negative: on G, with D as the batch edges. */
-    rc |= delta(o, del, nd, nthreads, want_rows, o->per_qe[1], &o->rows[1], &o->nrows[1]);
+    rc |= delta(o, del, nd, nthreads, want_rows, o->per_qe[1], &o->rows[1], &o->nrows[1], deadline, items);
     for (uint64_t i = 0; i < nd; i++) {
         adj_remove(&o->adj[del[i].x], del[i].y, del[i].l);
         adj_remove(&o->adj[del[i].y], del[i].x, del[i].l);
@@ -442,7 +516,7 @@ int oracle_apply(void *h, uint64_t nb, const uint32_t *bs, const uint32_t *bd, c
         adj_insert(&o->adj[ins[i].y], ins[i].x, ins[i].l);
     }
     /* Positive: on G', with I as the batch edges. */
-    rc |= delta(o, ins, ni, nthreads, want_rows, o->per_qe[0], &o->rows[0], &o->nrows[0]);
+    rc |= delta(o, ins, ni, nthreads, want_rows, o->per_qe[0], &o->rows[0], &o->nrows[0], deadline, items);
     o->pos = o->neg = 0;
     for (uint32_t i = 0; i < o->qm; i++) {
         o->pos += o->per_qe[0][i];
@@ -462,6 +536,23 @@ int oracle_apply(void *h, uint64_t nb, const uint32_t *bs, const uint32_t *bd, c
     free(ins);
     free(del);
     return rc;
+}
+
+int oracle_apply(void *h, uint64_t nb, const uint32_t *bs, const uint32_t *bd, const uint32_t *bl, const uint8_t *bdel,
+                 int nthreads, int want_rows, uint64_t *out, uint64_t *per_qe) {
+    return apply_impl(h, nb, bs, bd, bl, bdel, nthreads, want_rows, out, per_qe, 0.0, NULL);
+}
+
+/*
+ * Throughput sample: applies the batch to the graph like oracle_apply but stops counting
+ * once `max_seconds` have passed (the counts then cover a scattered subset of the work
+ * items); *items receives the number of (query edge, batch edge, orientation) items done.
+ */
+int oracle_apply_sample(void *h, uint64_t nb, const uint32_t *bs, const uint32_t *bd, const uint32_t *bl,
+                        const uint8_t *bdel, int nthreads, double max_seconds, uint64_t *out, uint64_t *items) {
+    uint64_t per[2 * MAXQE];
+    *items = 0;
+    return apply_impl(h, nb, bs, bd, bl, bdel, nthreads, 0, out, per, max_seconds, items);
 }
 
 /* Copies the sorted rows of the last batch (sign > 0 positive, < 0 negative); returns the count. */

@@ -40,6 +40,9 @@ def load():
     lib.oracle_apply.restype = ctypes.c_int
     lib.oracle_apply.argtypes = [ctypes.c_void_p, ctypes.c_uint64, u32p, u32p, u32p, u8p, ctypes.c_int, ctypes.c_int,
                                  u64p, u64p]
+    lib.oracle_apply_sample.restype = ctypes.c_int
+    lib.oracle_apply_sample.argtypes = [ctypes.c_void_p, ctypes.c_uint64, u32p, u32p, u32p, u8p, ctypes.c_int,
+                                        ctypes.c_double, u64p, u64p]
     lib.oracle_rows.restype = ctypes.c_uint64
     lib.oracle_rows.argtypes = [ctypes.c_void_p, ctypes.c_int, u32p, ctypes.c_uint64]
     lib.oracle_work.argtypes = [ctypes.c_void_p, u64p, u64p]
@@ -100,6 +103,22 @@ class Oracle:
             raise MemoryError("oracle_apply failed")
         return dict(pos=out[0], neg=out[1], ins=out[2], dels=out[3], per_qe_pos=list(per)[: self.qm],
                     per_qe_neg=list(per)[self.qm:])
+
+    def apply_sample(self, batch, max_seconds: float, threads: int = 0):
+        """Applies `batch`, counting for at most `max_seconds`; returns (matches, items_done)."""
+        threads = threads or (os.cpu_count() or 1)
+        s, d, l = _a(batch.src), _a(batch.dst), _a(batch.elabels)
+        dp = None
+        if batch.is_delete is not None:
+            dl = _a(batch.is_delete, np.uint8)
+            dp = _p(dl, ctypes.c_uint8)
+        out = (ctypes.c_uint64 * 4)()
+        items = ctypes.c_uint64()
+        rc = self.lib.oracle_apply_sample(self.h, len(s), _p(s), _p(d), _p(l), dp, threads, max_seconds, out,
+                                          ctypes.byref(items))
+        if rc != 0:
+            raise MemoryError("oracle_apply_sample failed")
+        return int(out[0] + out[1]), int(items.value)
 
     def rows(self, sign: int = 1) -> np.ndarray:
         n = self.lib.oracle_rows(self.h, sign, None, 0)
