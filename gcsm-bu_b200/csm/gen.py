@@ -28,6 +28,8 @@ def chung_lu(n: int, m: int, gamma: float, rng: np.random.Generator, cap: bool =
     w = (np.arange(n, dtype=np.float64) + 1.0) ** (-1.0 / (gamma - 1.0))
     w *= 2.0 * m / w.sum()
     if cap:
+        # Structural cutoff of the Chung-Lu model: w_i w_j / sum(w) is an edge probability, so
+        # no weight may exceed sqrt(sum(w)).
         w = np.minimum(w, np.sqrt(w.sum()))
     p = w / w.sum()
     cdf = np.cumsum(p)
@@ -240,16 +242,16 @@ CONFIGS = {
     "c1": dict(n=10_000, m=50_000, gamma=2.3, nvl=4, vzipf=None, nel=1, ezipf=None, cap=False, n_ins=5_000, n_del=0,
                batch=1024, queries=[("cycle4", 4)]),
     # Amazon-shaped: 400k vertices, 2.4M edges, 6 Zipf(1.0) labels, 240k updates (10% deletions).
-    "c2": dict(n=400_000, m=2_400_000, gamma=2.1, nvl=6, vzipf=1.0, nel=1, ezipf=None, cap=False, n_ins=216_000,
+    "c2": dict(n=400_000, m=2_400_000, gamma=2.1, nvl=6, vzipf=1.0, nel=1, ezipf=None, cap=True, n_ins=216_000,
                n_del=24_000, batch=65_536, queries=[("dense", 6)] * 5 + [("tree", 6)] * 5),
     # LiveJournal-shaped heavy-vertex stress: 4.8M vertices, 43M edges, 20 Zipf(1.2) labels.
     "c3": dict(n=4_800_000, m=43_000_000, gamma=1.9, nvl=20, vzipf=1.2, nel=1, ezipf=None, cap=True,
                n_ins=2_150_000, n_del=2_150_000, batch=1_000_000, queries=[("dense", 8)] * 4),
     # Batched multi-query: the Amazon-shaped graph, 64 queries of 4..12 vertices.
-    "c4": dict(n=400_000, m=2_400_000, gamma=2.1, nvl=6, vzipf=1.0, nel=1, ezipf=None, cap=False, n_ins=216_000,
+    "c4": dict(n=400_000, m=2_400_000, gamma=2.1, nvl=6, vzipf=1.0, nel=1, ezipf=None, cap=True, n_ins=216_000,
                n_del=24_000, batch=65_536, queries="mixed64"),
     # Serving: Netflow-shaped multi-label graph, 32 queries of 4..10 vertices.
-    "c5": dict(n=3_000_000, m=20_000_000, gamma=2.1, nvl=8, vzipf=None, nel=16, ezipf=1.1, cap=False,
+    "c5": dict(n=3_000_000, m=20_000_000, gamma=2.1, nvl=8, vzipf=None, nel=16, ezipf=1.1, cap=True,
                n_ins=700_000, n_del=300_000, batch=65_536, queries="mixed32"),
 }
 

@@ -65,6 +65,7 @@ struct DevTail {
     uint16_t key_rel[CSM_TAIL_MAXKEYS];
     uint8_t nmasks;                             // key subsets whose intersection size is used
     uint8_t nclasses;
+    uint8_t lane_par;                           // every mask is one key: count 32 prefixes per warp step
     uint16_t mask[CSM_TAIL_MAXMASKS];
     uint16_t class_term_begin[CSM_TAIL_MAXCLASSES + 1];  // into the plan's term list
 };

@@ -81,7 +81,8 @@ csm_status Engine::init() {
     CSM_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     for (auto &e : ev_) CSM_CUDA(cudaEventCreate(&e));
     warps_per_block_ = cfg_.warps_per_block > 0 && cfg_.warps_per_block <= 8 ? cfg_.warps_per_block : 8;
-    const int bps = cfg_.blocks_per_sm > 0 ? cfg_.blocks_per_sm : 4;
+    // Persistent launch: as many blocks as can be resident on every SM.
+    const int bps = cfg_.blocks_per_sm > 0 ? cfg_.blocks_per_sm : enum_blocks_per_sm(warps_per_block_);
     blocks_ = sm_count_ * bps;
     CSM_CUDA(dalloc(&d_ctrl_, 1));
     CSM_CUDA(dalloc(&d_misc_, 8));
@@ -561,7 +562,10 @@ csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
     P.ctrl = d_ctrl_;
     P.counts = d_counts_ + (phase == CSM_PHASE_INS ? np : 0);
     P.steal_min = cfg_.steal_chunk > 0 ? (uint32_t)cfg_.steal_chunk : 64u;
-    P.idle_limit = 1u << 18;
+    // An idle warp leaves as soon as no warp holds work; the bound (about a minute of
+    // polling) only ends the wait if that never happens.
+    P.idle_limit = 1u << 26;
+    P.ready_limit = 1u << 22;
     P.abort_flag = phase == CSM_PHASE_INS ? bs_.error : nullptr;
     P.rows = d_rows_;
     P.row_cap = row_cap_;

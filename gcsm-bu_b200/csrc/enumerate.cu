@@ -41,6 +41,7 @@ struct __align__(16) WarpState {
     uint32_t base[CSM_MAXQV];
     uint32_t poff[CSM_MAXQV][CSM_MAXBN];
     uint32_t psz[CSM_MAXQV][CSM_MAXBN];
+    uint32_t cur[CSM_MAXQV][CSM_MAXBN];   // per probe list: entries before it are below the next chunk
     uint32_t nlf[CSM_MAXQV];
     uint16_t oldm[CSM_MAXQV];
     uint8_t nbuf[CSM_MAXQV];
@@ -52,6 +53,11 @@ struct __align__(16) WarpState {
     uint32_t t_flag[CSM_TAIL_MAXKEYS];
     uint32_t t_excl[CSM_TAIL_MAXKEYS];
     unsigned long long msize[CSM_TAIL_MAXMASKS];
+    // Lane-parallel tail: per key whose parent is matched before the counting level, its
+    // list and the list size left after the flag rule and the shared prefix.
+    uint32_t ts_off[CSM_TAIL_MAXKEYS];
+    uint32_t ts_size[CSM_TAIL_MAXKEYS];
+    uint32_t ts_base[CSM_TAIL_MAXKEYS];
     uint32_t item_plan;
     uint32_t item_depth;
     uint32_t item_lo;
@@ -74,6 +80,129 @@ __device__ __forceinline__ const uint32_t *bitmap(const EnumParams &P, uint32_t 
     return P.bits + (size_t)id * P.words;
 }
 
+// First index in [lo, hi) of the sorted list L whose entry is >= key2, found by the whole warp
+// with 32-ary search: each round reads 32 evenly spaced entries and keeps the bracket that
+// holds the answer, so a list of n entries costs about log32(n) dependent reads.
+__device__ __forceinline__ uint32_t warp_lower_bound(const uint32_t *L, uint32_t lo, uint32_t hi, uint32_t key2,
+                                                     uint32_t lane) {
+    while (hi - lo > 32) {
+        const uint32_t step = (hi - lo + 31) / 32;
+        const uint32_t p = lo + (lane + 1) * step - 1;
+        const uint32_t v = p < hi ? __ldg(L + p) : 0xFFFFFFFFu;
+        const uint32_t c = __popc(__ballot_sync(0xffffffffu, v < key2));
+        const uint32_t nhi = lo + (c + 1) * step - 1;
+        lo = lo + c * step;
+        if (nhi < hi) hi = nhi;
+    }
+    const uint32_t p = lo + lane;
+    const uint32_t v = p < hi ? __ldg(L + p) : 0xFFFFFFFFu;
+    return lo + __popc(__ballot_sync(0xffffffffu, v < key2));
+}
+
+// Lower bound of key2 among the 32 register-held window entries (sorted, padded with ~0).
+__device__ __forceinline__ uint32_t shfl_lower_bound(uint32_t win, uint32_t key2) {
+    uint32_t pos = 0;
+#pragma unroll
+    for (uint32_t step = 16; step > 0; step >>= 1)
+        if (__shfl_sync(0xffffffffu, win, pos + step - 1) < key2) pos += step;
+    return pos;
+}
+
+// Flagged entries of list (rel, x) in this phase (batch edges of that list), 0 if none.
+__device__ __forceinline__ uint32_t flagged_in_list(const EnumParams &P, uint32_t rel, uint32_t x) {
+    const unsigned long long lk = P.kl.list_key(rel, x);
+    const uint32_t h = find_list_head(P.keys, P.m, P.kl, lk);
+    return (h < P.m && P.kl.list_of(__ldg(P.keys + h)) == lk) ? __ldg(P.seg_flagged + h) : 0u;
+}
+
+// Lane-parallel tail, shared part: for the counting level d = tail_start - 1 and the current
+// prefix f[0..d-1], every tail key whose parent is matched before depth d gets its list and
+// the number of its entries the leaves may still use given that prefix.
+__device__ void prep_tail_shared(WarpState &S, const EnumParams &P, const DevPlan *pl, uint32_t d) {
+    const uint32_t lane = lane_id();
+    const DevTail *T = &pl->tail;
+    const uint32_t nkeys = __ldg(&T->nkeys);
+    if (lane < nkeys) {
+        const uint32_t pd = __ldg(&T->key_parent[lane]);
+        if (pd < d) {
+            const uint32_t rel = __ldg(&T->key_rel[lane]);
+            const bool old = __ldg(&T->key_old[lane]) != 0;
+            const uint32_t x = S.f[pd];
+            const uint2 ms = __ldg(P.g.meta + (size_t)rel * P.g.V + x);
+            uint32_t left = ms.y - (old ? flagged_in_list(P, rel, x) : 0u);
+            for (uint32_t j = 0; j < d; j++) {
+                if (j == pd) continue;
+                const uint32_t e = find_entry(P.g.pool + ms.x, ms.y, S.f[j]);
+                if (e != 0xFFFFFFFFu && !(old && (e & 1u))) left--;
+            }
+            S.ts_off[lane] = ms.x;
+            S.ts_size[lane] = ms.y;
+            S.ts_base[lane] = left;
+        }
+    }
+    __syncwarp();
+}
+
+// Lane-parallel tail, per lane: the tail count of the prefix f[0..d-1] + v, where v is this
+// lane's candidate at depth d (for d == 1 the prefix is the seed edge (x0, v)).  Only for
+// plans whose masks are single keys (no list intersections).
+__device__ unsigned long long tail_count_lane(const WarpState &S, const EnumParams &P, const DevPlan *pl,
+                                              uint32_t d, uint32_t x0, uint32_t v, unsigned long long &probes) {
+    const DevTail *T = &pl->tail;
+    const uint32_t nkeys = __ldg(&T->nkeys);
+    uint32_t ksize[CSM_TAIL_MAXKEYS];
+#pragma unroll
+    for (uint32_t k = 0; k < CSM_TAIL_MAXKEYS; k++) {
+        if (k >= nkeys) break;
+        const uint32_t pd = __ldg(&T->key_parent[k]);
+        const uint32_t rel = __ldg(&T->key_rel[k]);
+        const bool old = __ldg(&T->key_old[k]) != 0;
+        uint32_t left;
+        if (pd < d && d >= 2) {
+            // Shared list: only this lane's candidate may still sit in it.
+            left = S.ts_base[k];
+            const uint32_t e = find_entry(P.g.pool + S.ts_off[k], S.ts_size[k], v);
+            probes++;
+            if (e != 0xFFFFFFFFu && !(old && (e & 1u))) left--;
+        } else {
+            const uint32_t x = (pd == d) ? v : x0;  // d >= 2: pd == d; d == 1: parent 0 or 1
+            const uint2 ms = __ldg(P.g.meta + (size_t)rel * P.g.V + x);
+            left = ms.y - (old ? flagged_in_list(P, rel, x) : 0u);
+            for (uint32_t j = 0; j <= d; j++) {
+                if (j == pd) continue;
+                const uint32_t z = (j == d) ? v : (d == 1 ? x0 : S.f[j]);
+                const uint32_t e = find_entry(P.g.pool + ms.x, ms.y, z);
+                probes++;
+                if (e != 0xFFFFFFFFu && !(old && (e & 1u))) left--;
+            }
+        }
+        ksize[k] = left;
+    }
+    // Masks are single keys here: mask mi stands for key ffs(mask) - 1.
+    unsigned long long total = 1;
+    const DevTailTerm *terms = P.terms + pl->term_begin;
+    const uint32_t nclasses = __ldg(&T->nclasses);
+    for (uint32_t c = 0; c < nclasses; c++) {
+        unsigned long long s = 0;
+        const uint32_t tb = __ldg(&T->class_term_begin[c]), te = __ldg(&T->class_term_begin[c + 1]);
+        for (uint32_t t = tb; t < te; t++) {
+            unsigned long long prod = (unsigned long long)__ldg(&terms[t].coef);
+            const uint32_t nf = __ldg(&terms[t].nf);
+            for (uint32_t j = 0; j < nf; j++) {
+                const uint32_t mk = __ldg(&T->mask[__ldg(&terms[t].f[j])]);
+                uint32_t sz = 0;
+#pragma unroll
+                for (uint32_t k = 0; k < CSM_TAIL_MAXKEYS; k++)
+                    if (mk == (1u << k)) sz = ksize[k];
+                prod *= sz;
+            }
+            s += prod;
+        }
+        total *= s;
+    }
+    return total;
+}
+
 // Sets up level d for the current prefix: the backward-neighbour lists and the pivot.
 __device__ void enter_level(WarpState &S, const EnumParams &P, const DevPlan *pl, uint32_t d, uint32_t rlo,
                             uint32_t rhi) {
@@ -88,6 +217,7 @@ __device__ void enter_level(WarpState &S, const EnumParams &P, const DevPlan *pl
         const uint2 ms = __ldg(P.g.meta + (size_t)rel * P.g.V + v);
         S.poff[d][lane] = ms.x;
         S.psz[d][lane] = ms.y;
+        S.cur[d][lane] = 0;
         sz = ms.y;
     }
     const uint32_t piv = warp_min_index(sz, lane);
@@ -105,6 +235,7 @@ __device__ void enter_level(WarpState &S, const EnumParams &P, const DevPlan *pl
         S.nlf[d] = __ldg(&lv->nlf_bitmap);
     }
     __syncwarp();
+    if (d + 1 == pl->tail_start && pl->tail_start < pl->n && pl->tail.lane_par) prep_tail_shared(S, P, pl, d);
 }
 
 // Number of injective assignments of the tail leaves for the full prefix f[0..E-1].
@@ -254,7 +385,10 @@ __device__ bool try_donate(WarpState &S, const EnumParams &P, const DevPlan *pl,
             const uint32_t slot = reserve_slots(P, 1);
             if (slot == 0xFFFFFFFFu) return false;
             publish_item(P, slot, S.item_plan, l == 1 ? 0u : l, mid, hi, S.f, l == 1 ? 0u : l, false, 0, 0);
-            if (lane == 0) S.hi[l] = mid;
+            if (lane == 0) {
+                S.hi[l] = mid;
+                atomicAdd(&P.ctrl->donations, 1ull);
+            }
             __syncwarp();
             return true;
         }
@@ -273,7 +407,10 @@ __device__ bool try_donate(WarpState &S, const EnumParams &P, const DevPlan *pl,
                     publish_item(P, slot + j, S.item_plan, l + 1, 0, 0xFFFFFFFFu, S.f, l, true, c, l);
                 }
             }
-            if (lane == 0) S.nbuf[l] = (uint8_t)ps;
+            if (lane == 0) {
+                S.nbuf[l] = (uint8_t)ps;
+                atomicAdd(&P.ctrl->donations, (unsigned long long)cnt);
+            }
             __syncwarp();
             return true;
         }
@@ -303,7 +440,7 @@ __device__ int claim_item(WarpState &S, const EnumParams &P, unsigned int &err) 
             const uint32_t ep = P.ctrl->epoch;
             unsigned int spins = 0;
             while (*rd != ep) {
-                if (++spins > P.idle_limit) {
+                if (++spins > P.ready_limit) {
                     err |= CSM_ERRBIT_TIMEOUT;
                     slot = 0xFFFFFFFEu;
                     break;
@@ -480,12 +617,33 @@ __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, unsign
             }
             for (uint32_t k = 0; ok && k < d; k++) ok = S.f[k] != cand;
             if (ok) ok = test_bit(bitmap(P, S.nlf[d]), cand);
+            // Membership in the other backward lists.  The chunk's candidates ascend, so each
+            // list keeps a cursor; the warp brackets the chunk's window in the list and, when
+            // the window fits in a warp, checks membership by shuffles over the window.
             const uint32_t nbn = S.nbn[d];
-            for (uint32_t k = 0; ok && k < nbn; k++) {
+            const uint32_t vmask = __ballot_sync(0xffffffffu, idx < S.hi[d]);
+            const uint32_t target = __shfl_sync(0xffffffffu, cand, 31 - __clz(vmask));
+            for (uint32_t k = 0; k < nbn; k++) {
                 if (k == piv) continue;
-                const uint32_t e = find_entry(P.g.pool + S.poff[d][k], S.psz[d][k], cand);
-                probes++;
-                ok = e != 0xFFFFFFFFu && !(((oldm >> k) & 1u) && (e & 1u));
+                if (!__any_sync(0xffffffffu, ok)) break;
+                const uint32_t *L = P.g.pool + S.poff[d][k];
+                const uint32_t c0 = S.cur[d][k];
+                const uint32_t hi = warp_lower_bound(L, c0, S.psz[d][k], (target + 1) << 1, lane);
+                const uint32_t W = hi - c0;
+                uint32_t e = 0xFFFFFFFFu;
+                if (W <= 32) {
+                    const uint32_t win = lane < W ? __ldg(L + c0 + lane) : 0xFFFFFFFFu;
+                    const uint32_t pos = shfl_lower_bound(win, cand << 1);
+                    const uint32_t got = __shfl_sync(0xffffffffu, win, pos);
+                    if ((got >> 1) == cand && got != 0xFFFFFFFFu) e = got;
+                } else if (ok) {
+                    e = find_entry(L + c0, W, cand);
+                }
+                if (ok) {
+                    probes++;
+                    ok = e != 0xFFFFFFFFu && !(((oldm >> k) & 1u) && (e & 1u));
+                }
+                if (lane == 0) S.cur[d][k] = hi;
             }
         }
         __syncwarp();
@@ -516,6 +674,20 @@ __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, unsign
                 }
             }
             __syncwarp();
+        } else if (d + 1 == E && E < n && pl->tail.lane_par) {
+            // Counting level before the tail: every surviving lane sizes its own tail.
+            unsigned long long t = 0;
+            if (ok) {
+                if (d == 1) {
+                    const unsigned long long key = __ldg(P.keys + cand);
+                    t = tail_count_lane(S, P, pl, 1, P.kl.src(key), P.kl.dst(key), probes);
+                } else {
+                    t = tail_count_lane(S, P, pl, d, 0, cand, probes);
+                }
+            }
+            for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+            cnt += t;
+            tails += __popc(mask);
         } else if (d + 1 == n) {
             if (P.mode == CSM_ENUM_MODE_ROWS) {
                 const uint32_t c = __popc(mask);
@@ -551,7 +723,7 @@ __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, unsign
     return cnt;
 }
 
-__global__ void __launch_bounds__(256) k_enumerate(EnumParams P) {
+__global__ void __launch_bounds__(256, 4) k_enumerate(EnumParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
     WarpState &S = reinterpret_cast<WarpState *>(smem)[threadIdx.x >> 5];
     const uint32_t lane = lane_id();
@@ -719,6 +891,15 @@ __global__ void k_expand_bound(EnumParams P, const WorkItem *items, const unsign
 }  // namespace
 
 size_t enum_smem_bytes(int warps_per_block) { return sizeof(WarpState) * (size_t)warps_per_block; }
+
+int enum_blocks_per_sm(int warps_per_block) {
+    const size_t smem = enum_smem_bytes(warps_per_block);
+    cudaFuncSetAttribute(k_enumerate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_enumerate, warps_per_block * 32, smem) != cudaSuccess)
+        return 1;
+    return nb > 0 ? nb : 1;
+}
 
 void launch_enumerate(const EnumParams &p, int blocks, int warps_per_block, cudaStream_t s) {
     const size_t smem = enum_smem_bytes(warps_per_block);

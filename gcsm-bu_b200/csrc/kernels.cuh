@@ -104,7 +104,8 @@ struct EnumParams {
     unsigned long long expand_cap;
     uint32_t donate;
     uint32_t steal_min;
-    uint32_t idle_limit;
+    uint32_t idle_limit;             // polls of an idle warp waiting for donated work
+    uint32_t ready_limit;            // polls of a claimed slot whose item is being written
     const unsigned int *abort_flag;  // nonzero: the batch update failed, skip enumeration
 };
 
@@ -114,6 +115,7 @@ struct EnumParams {
 #define CSM_ENUM_MODE_EXPAND 2
 
 size_t enum_smem_bytes(int warps_per_block);
+int enum_blocks_per_sm(int warps_per_block);  // resident blocks per SM of the enumeration kernel
 void launch_enumerate(const EnumParams &p, int blocks, int warps_per_block, cudaStream_t s);
 void launch_seed_tickets(const DevPlan *plans, uint32_t nplans, const unsigned long long *keys, uint32_t m,
                          KeyLayout kl, uint32_t *seed_lo, uint32_t *ticket_prefix, EnumControl *ctrl,

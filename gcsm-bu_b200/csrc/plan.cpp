@@ -404,7 +404,11 @@ bool build_tail(const Query &q, const HostPlan &hp, int qe, const RelOf &rel_of,
     tail.class_term_begin[c] = (uint16_t)terms.size();
     if (masks.size() > CSM_TAIL_MAXMASKS) return false;
     tail.nmasks = (uint8_t)masks.size();
-    for (size_t k = 0; k < masks.size(); k++) tail.mask[k] = masks[k];
+    tail.lane_par = 1;
+    for (size_t k = 0; k < masks.size(); k++) {
+        tail.mask[k] = masks[k];
+        if (__builtin_popcount(masks[k]) != 1) tail.lane_par = 0;
+    }
     return true;
 }
 
