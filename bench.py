@@ -159,67 +159,77 @@ def max_over_ranks(x, world, device=None):
     return float(t.item())
 
 
-def oracle_sample(w, seq, budget_s):
-    """Runs the CPU oracle (all host threads) over the step batches: each batch is applied in
-    full, and its counting stops once its share of the time budget is spent (the counted part
-    is a scattered subset of the batch's work items).  Returns (matches, seconds, items, per-step s)."""
+def oracle_sample(w, steps, budget_s, warmup=0):
+    """The CPU oracle (all host threads) over (query, batch) steps: every batch is applied in
+    full to its query's oracle, and the counting of a step stops once its share of the time
+    budget is spent (the counted part is a scattered subset of the step's work items).  The
+    first `warmup` steps only advance the streams.  Returns (matches, seconds, items, per-step s)."""
     from oracle import Oracle
     threads = os.cpu_count() or 1
     oracles = [Oracle(q, w.data) for q in w.queries]
-    per_query = budget_s / max(1, len(seq)) / max(1, len(oracles))
+    per_step = budget_s / max(1, len(steps) - warmup)
     matches, t_total, items, lat = 0, 0.0, 0, []
-    for b in seq:
-        t_step = 0.0
-        for o in oracles:
-            t0 = time.perf_counter()
-            m, it = o.apply_sample(b, per_query, threads=threads)
-            t_step += time.perf_counter() - t0
-            matches += m
-            items += it
-        lat.append(t_step)
-        t_total += t_step
+    for i, (qi, b) in enumerate(steps):
+        if i < warmup:
+            oracles[qi].apply_sample(b, 1e-3, threads=threads)
+            continue
+        t0 = time.perf_counter()
+        m, it = oracles[qi].apply_sample(b, per_step, threads=threads)
+        dt = time.perf_counter() - t0
+        matches += m
+        items += it
+        lat.append(dt)
+        t_total += dt
     for o in oracles:
         o.close()
     return matches, t_total, items, lat
 
 
 def cpu_baseline(w, args, budget_s=20.0):
-    seq = step_batches(w, 2)
-    matches, t, items, _ = oracle_sample(w, seq, budget_s)
+    steps = step_plan(w, len(w.queries))
+    matches, t, items, _ = oracle_sample(w, steps, budget_s)
     threads = os.cpu_count() or 1
     return {"value": matches / t if t else None, "unit": "matches/s", "cores": threads, "kind": "port",
-            "sample": f"CPU oracle on the first 2 batches x {len(w.queries)} queries, counting capped at "
-                      f"{budget_s / 2 / len(w.queries):.1f} s per (batch, query): {items} seed items, "
+            "sample": f"CPU oracle, first batch x {len(w.queries)} queries, counting capped at "
+                      f"{budget_s / len(steps):.1f} s per (query, batch): {items} seed items, "
                       f"{matches} matches in {t:.1f} s"}
 
 
 def run_reference(args, w, world, rank):
-    """The CPU implementation of the path (the oracle port; the reference itself is GPU-only)
-    on all host threads: every step is a time-bounded sample of that step's batch."""
+    """The CPU implementation of the path (the oracle port; the reference itself runs only on
+    a GPU) on all host threads, over the same (query, batch) steps as the GPU arm; each step is
+    a time-bounded sample of its work."""
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    seq = step_batches(w, args.warmup + args.steps)
-    oracle_sample(w, seq[: args.warmup], 5.0)
+    plan = step_plan(w, args.warmup + args.steps)
     budget = float(os.environ.get("CSM_REF_BUDGET_S", "150"))
-    matches, t_total, items, lat = oracle_sample(w, seq[args.warmup:], budget)
-    upd = sum(len(b.src) for b in seq[args.warmup:])
+    matches, t_total, items, lat = oracle_sample(w, plan, budget, warmup=args.warmup)
     value = matches / t_total if t_total else 0.0
     out = {
         "metric": "incremental matches/sec", "value": value, "unit": "matches/s", "impl": "reference",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": f"{w.name}: Chung-Lu {len(w.data.vlabels)} vertices, "
-                               f"{len(w.data.src)} initial edges, {len(w.queries)} standing queries, "
-                               f"batches of {w.batch_size} updates (stream then its inverse)",
+        "config": {"workload": f"{w.name}: Chung-Lu {len(w.data.vlabels)} vertices, {len(w.data.src)} initial edges;"
+                               f" step = one {w.batch_size}-update batch for one of {len(w.queries)} standing"
+                               " queries (stream, then its inverse)",
                    "batch_size": w.batch_size, "queries": len(w.queries), "parallelism": "host threads"},
         "cpu_baseline": {"value": value, "unit": "matches/s", "cores": threads, "kind": "port",
-                         "sample": f"{args.steps} steps x {len(w.queries)} queries, each batch applied in full "
-                                   f"with counting capped at {budget / args.steps / len(w.queries):.1f} s per "
-                                   f"(step, query): {items} seed items, {matches} matches"},
+                         "sample": f"{args.steps} (query, batch) steps, each batch applied in full with counting "
+                                   f"capped at {budget / args.steps:.1f} s per step: {items} seed items, "
+                                   f"{matches} matches"},
         "e2e": {"value": value, "unit": "matches/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out))
+
+
+def step_plan(w, count):
+    """Step i applies stream batch i // Q to standing query i % Q: the plain per-query path, one
+    engine per query (the reference runs one csmg process per query), every query seeing the
+    stream in order."""
+    Q = len(w.queries)
+    seq = step_batches(w, (count + Q - 1) // Q + 1)
+    return [(i % Q, seq[i // Q]) for i in range(count)]
 
 
 def run_ours(args, w, world, rank, local):
@@ -228,10 +238,12 @@ def run_ours(args, w, world, rank, local):
     import csm
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    eng = csm.Engine(device=local, algorithm=0, search_strategy=args.strategy, max_batch=w.batch_size)
+    engines = []
     for q in w.queries:
+        eng = csm.Engine(device=local, algorithm=0, search_strategy=args.strategy, max_batch=w.batch_size)
         eng.load_query(q)
-    eng.load_graph(w.data)
+        eng.load_graph(w.data)
+        engines.append(eng)
     stream = torch.cuda.current_stream(dev)
     cache = {}
 
@@ -244,44 +256,45 @@ def run_ours(args, w, world, rank, local):
                                          b.elabels.astype(np.int32), dl.astype(np.uint8)))
         return cache[key]
 
-    def apply_dev(b):
+    def apply_dev(qi, b):
         s, d, l, dl = on_device(b)
-        return eng.apply_device(len(b.src), s.data_ptr(), d.data_ptr(), l.data_ptr(), dl.data_ptr(),
-                                stream.cuda_stream)
+        return engines[qi].apply_device(len(b.src), s.data_ptr(), d.data_ptr(), l.data_ptr(), dl.data_ptr(),
+                                        stream.cuda_stream)[0]
 
-    seq = step_batches(w, args.warmup + 2 * args.steps)
-    warm, timed, timed_e2e = seq[: args.warmup], seq[args.warmup: args.warmup + args.steps], seq[args.warmup + args.steps:]
-    for b in warm + timed + timed_e2e:
+    plan = step_plan(w, args.warmup + 2 * args.steps)
+    warm, timed, timed_e2e = plan[: args.warmup], plan[args.warmup: args.warmup + args.steps], plan[args.warmup + args.steps:]
+    for _, b in plan:
         on_device(b)
-    for b in warm:
-        apply_dev(b)
+    for qi, b in warm:
+        apply_dev(qi, b)
     torch.cuda.synchronize(dev)
-    eng.reset_stats()
+    for e in engines:
+        e.reset_stats()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     matches, upd, lat = 0, 0, []
     barrier(world)
     torch.cuda.synchronize(dev)
     with ClockSampler(local) as clk:
         ev0.record(stream)
-        for b in timed:
-            res = apply_dev(b)
-            matches += sum(r.positive + r.negative for r in res)
-            upd += int(res[0].inserted + res[0].deleted)
-            lat.append(res[0].latency_ns / 1e6)
+        for qi, b in timed:
+            r = apply_dev(qi, b)
+            matches += r.positive + r.negative
+            upd += len(b.src)
+            lat.append(r.latency_ns / 1e6)
         ev1.record(stream)
         torch.cuda.synchronize(dev)
     barrier(world)
     t = ev0.elapsed_time(ev1) / 1e3
     tmax = max_over_ranks(t, world, dev)
-    st = eng.stats()
+    sts = [e.stats() for e in engines]
 
-    # End to end: host (pinned) update arrays through csm_apply_batch, next steps of the cycle.
+    # End to end: host (pinned) update arrays through csm_apply_batch, the next steps.
     pinned = {}
-    for b in timed_e2e:
+    for _, b in timed_e2e:
         if id(b) not in pinned:
             arrs = []
-            for a, dt in ((b.src, torch.int32), (b.dst, torch.int32), (b.elabels, torch.int32)):
-                h = torch.empty(len(a), dtype=dt, pin_memory=True)
+            for a in (b.src, b.dst, b.elabels):
+                h = torch.empty(len(a), dtype=torch.int32, pin_memory=True)
                 h.numpy()[:] = a.view(np.int32)
                 arrs.append(h)
             dl = b.is_delete if b.is_delete is not None else np.zeros(len(b.src), dtype=np.uint8)
@@ -293,54 +306,56 @@ def run_ours(args, w, world, rank, local):
     barrier(world)
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
-    for b in timed_e2e:
+    for qi, b in timed_e2e:
         s, d, l, dl = pinned[id(b)]
-        res = eng.apply(csm.Batch(s.numpy().view(np.uint32), d.numpy().view(np.uint32), l.numpy().view(np.uint32),
-                                  dl.numpy()))
-        matches_e2e += sum(r.positive + r.negative for r in res)
+        r = engines[qi].apply(csm.Batch(s.numpy().view(np.uint32), d.numpy().view(np.uint32),
+                                        l.numpy().view(np.uint32), dl.numpy()))[0]
+        matches_e2e += r.positive + r.negative
         h2d += 13 * len(b.src)
     t_e2e = time.perf_counter() - t0
     t_e2e_max = max_over_ranks(t_e2e, world, dev)
-    pool_mb = st.pool_capacity * 4 / 2 ** 20
-    eng.close()
+    pool_mb = max(st.pool_capacity for st in sts) * 4 / 2 ** 20
+    for e in engines:
+        e.close()
     if rank != 0:
         return
     peak, peak_kind = measured_peaks()
-    alg_bytes = 4.0 * (st.enum_scan_entries + st.enum_probes + st.enum_tail_lists)
-    enum_s = st.enum_ns / 1e9
-    launches = max(1, st.enum_launches)
+    scan = sum(st.enum_scan_entries for st in sts)
+    probes = sum(st.enum_probes for st in sts)
+    tails = sum(st.enum_tail_lists for st in sts)
+    enum_s = sum(st.enum_ns for st in sts) / 1e9
+    apply_s = sum(st.apply_ns for st in sts) / 1e9
+    launches = max(1, sum(st.enum_launches for st in sts))
+    alg_bytes = 4.0 * (scan + probes + tails)
     achieved = alg_bytes / enum_s / 1e9 if enum_s > 0 else 0.0
     traffic = profile_traffic()
-    clocks = clk.summary()
     out = {
         "metric": "incremental matches/sec", "value": world * matches / tmax, "unit": "matches/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tmax / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": f"{w.name}: Chung-Lu {len(w.data.vlabels)} vertices, {len(w.data.src)} initial edges,"
-                               f" {len(w.queries)} standing queries, batches of {w.batch_size} updates"
-                               " (stream then its inverse)",
+        "config": {"workload": f"{w.name}: Chung-Lu {len(w.data.vlabels)} vertices, {len(w.data.src)} initial edges;"
+                               f" step = one {w.batch_size}-update batch for one of {len(w.queries)} standing"
+                               " queries (stream, then its inverse)",
                    "batch_size": w.batch_size, "queries": len(w.queries), "search_strategy": args.strategy,
                    "parallelism": f"replicas x{world}",
-                   "l2": f"inputs larger than L2 (adjacency pool {pool_mb:.0f} MiB, 126 MB L2)"},
+                   "l2": f"inputs larger than L2 (adjacency pool {pool_mb:.0f} MiB per engine, 126 MB L2)"},
         "update_edges_per_s": world * upd / tmax,
         "p50_batch_ms": float(np.percentile(lat, 50)), "p99_batch_ms": float(np.percentile(lat, 99)),
         "matches_per_step": matches / args.steps,
         "e2e": {"value": world * matches_e2e / t_e2e_max, "unit": "matches/s",
-                "h2d_bytes_per_step": h2d // max(1, len(timed_e2e)),
-                "d2h_bytes_per_step": 64 * len(w.queries)},
-        "gpu_launches": int(st.kernel_launches),
+                "h2d_bytes_per_step": h2d // max(1, len(timed_e2e)), "d2h_bytes_per_step": 64},
+        "gpu_launches": int(sum(st.kernel_launches for st in sts)),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": f"{peak_kind} hbm_gbs",
                      "kernel": "k_enumerate",
                      "algorithmic_bytes_per_launch": alg_bytes / launches,
                      "avg_launch_ms": 1e3 * enum_s / launches,
                      "traffic": traffic.get("dram_bytes_per_launch") if traffic else None},
-        "phase_ms": {"enumerate": 1e3 * enum_s / args.steps, "apply": st.apply_ns / 1e6 / args.steps},
-        "clocks": clocks,
+        "phase_ms_per_step": {"enumerate": 1e3 * enum_s / args.steps, "apply": 1e3 * apply_s / args.steps},
+        "clocks": clk.summary(),
     }
     if world == 1 and not args.no_cpu_baseline:
-        cb, _, _ = cpu_baseline(w, args)
-        out["cpu_baseline"] = cb
+        out["cpu_baseline"] = cpu_baseline(w, args)
     print(json.dumps(out))
 
 

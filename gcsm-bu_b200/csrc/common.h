@@ -104,7 +104,7 @@ struct EnumControl {
     unsigned long long nticket;       // total tickets
     unsigned int q_write;             // donation slots reserved
     unsigned int q_read;              // donation slots claimed
-    unsigned int hungry;              // warps waiting for work
+    unsigned int hungry;              // outstanding work requests of idle warps
     unsigned int active;              // warps holding work
     unsigned int error;               // bit 0 timeout, bit 1 output overflow, bit 2 queue overflow
     unsigned int epoch;               // launch epoch, marks ready slots

@@ -81,8 +81,11 @@ csm_status Engine::init() {
     CSM_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     for (auto &e : ev_) CSM_CUDA(cudaEventCreate(&e));
     warps_per_block_ = cfg_.warps_per_block > 0 && cfg_.warps_per_block <= 8 ? cfg_.warps_per_block : 8;
-    // Persistent launch: as many blocks as can be resident on every SM.
-    const int bps = cfg_.blocks_per_sm > 0 ? cfg_.blocks_per_sm : enum_blocks_per_sm(warps_per_block_);
+    // Persistent launch: never more blocks than can be resident at once.  Warps that run out
+    // of work wait for the others while any warp holds work, so a block that could only start
+    // after resident blocks exit would stall the launch until the idle bound runs out.
+    const int resident = enum_blocks_per_sm(warps_per_block_);
+    const int bps = cfg_.blocks_per_sm > 0 && cfg_.blocks_per_sm < resident ? cfg_.blocks_per_sm : resident;
     blocks_ = sm_count_ * bps;
     CSM_CUDA(dalloc(&d_ctrl_, 1));
     CSM_CUDA(dalloc(&d_misc_, 8));
@@ -337,7 +340,7 @@ csm_status Engine::load_graph(uint32_t nv, const uint32_t *vlabel, uint64_t ne, 
     h_counts_ = nullptr;
     CSM_CUDA(cudaMallocHost(&h_counts_, sizeof(unsigned long long) * (2 * np + 32)));
     // Donation queue and the semi-BFS frontier.
-    qcap_ = 1u << 20;
+    qcap_ = 1u << 21;
     CSM_CUDA(dalloc(&d_queue_, qcap_));
     CSM_CUDA(dalloc(&d_ready_, qcap_));
     CSM_CUDA(cudaMemset(d_ready_, 0, sizeof(uint32_t) * qcap_));
@@ -564,7 +567,7 @@ csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
     P.steal_min = cfg_.steal_chunk > 0 ? (uint32_t)cfg_.steal_chunk : 64u;
     // An idle warp leaves as soon as no warp holds work; the bound (about a minute of
     // polling) only ends the wait if that never happens.
-    P.idle_limit = 1u << 26;
+    P.idle_limit = 1u << 24;
     P.ready_limit = 1u << 22;
     P.abort_flag = phase == CSM_PHASE_INS ? bs_.error : nullptr;
     P.rows = d_rows_;

@@ -18,7 +18,7 @@
 // embedding is counted exactly once, at the largest query-edge index it maps to a batch edge.
 //
 // Load balance: warps first take seed chunks from a ticket counter.  A warp that runs out of
-// work registers as hungry; busy warps that see hungry warps split off part of their pending
+// work posts a request; a busy warp that takes a request splits off part of its pending
 // work (the upper half of a candidate range, or buffered sibling candidates) into a global
 // queue.  Every wait is bounded; a warp never waits on another warp's progress to finish its
 // own items, so exhausting a bound only costs balance, never a result.
@@ -561,10 +561,15 @@ __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, unsign
 
     while (true) {
         if (P.donate && ((++iter & 7u) == 0)) {
-            unsigned int h = 0;
-            if (lane == 0) h = *(volatile unsigned int *)&P.ctrl->hungry;
-            h = __shfl_sync(0xffffffffu, h, 0);
-            if (h > 0) try_donate(S, P, pl, L0, d);
+            // Each idle warp posts one request; a busy warp that takes a request splits off
+            // one piece of its pending work (and hands the request back if it has none).
+            unsigned int granted = 0;
+            if (lane == 0) {
+                const unsigned int h = *(volatile unsigned int *)&P.ctrl->hungry;
+                granted = h > 0 && atomicCAS(&P.ctrl->hungry, h, h - 1) == h;
+            }
+            granted = __shfl_sync(0xffffffffu, granted, 0);
+            if (granted && !try_donate(S, P, pl, L0, d) && lane == 0) atomicAdd(&P.ctrl->hungry, 1u);
         }
         if (S.pos[d] < S.nbuf[d]) {
             // Descend into the next buffered candidate.
@@ -749,21 +754,11 @@ __global__ void __launch_bounds__(256, 4) k_enumerate(EnumParams P) {
             bool resumed = false;
             for (uint32_t it = 0; it < P.idle_limit; it++) {
                 const int c = claim_item(S, P, err);
-                if (c != 0) {
-                    if (lane == 0) {
-                        atomicAdd(&P.ctrl->active, 1u);
-                        atomicSub(&P.ctrl->hungry, 1u);
-                    }
+                if (c < 0) continue;  // null slot
+                if (c > 0) {
+                    if (lane == 0) atomicAdd(&P.ctrl->active, 1u);
                     __syncwarp();
-                    if (c > 0) resumed = true;
-                    else {
-                        if (lane == 0) {
-                            atomicSub(&P.ctrl->active, 1u);
-                            atomicAdd(&P.ctrl->hungry, 1u);
-                        }
-                        __syncwarp();
-                        continue;
-                    }
+                    resumed = true;
                     break;
                 }
                 unsigned int act = 0, qr = 0, qw = 0;
@@ -779,10 +774,7 @@ __global__ void __launch_bounds__(256, 4) k_enumerate(EnumParams P) {
                 if (act == 0 && qr >= qw) break;
                 __nanosleep(512);
             }
-            if (!resumed) {
-                if (lane == 0) atomicSub(&P.ctrl->hungry, 1u);
-                break;
-            }
+            if (!resumed) break;
         }
         const unsigned long long c = run_item(S, P, scans, probes, tails, err);
         if (lane == 0 && c) atomicAdd(P.counts + S.item_plan, c);
