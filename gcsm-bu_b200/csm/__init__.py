@@ -36,7 +36,7 @@ ERRORS = {
 # Every symbol declared in include/csm.h.
 EXPORTED = [
     "csm_default_config", "csm_create", "csm_destroy", "csm_load_query", "csm_load_graph",
-    "csm_apply_batch", "csm_apply_batch_device", "csm_get_edge_counts", "csm_get_embeddings",
+    "csm_apply_batch", "csm_apply_batch_device", "csm_apply_batch_device_static", "csm_get_edge_counts", "csm_get_embeddings",
     "csm_free", "csm_describe_plan", "csm_get_stats", "csm_reset_stats", "csm_device_memory",
     "csm_last_error", "csm_version",
 ]
@@ -113,6 +113,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.csm_load_graph.argtypes = [vp, ctypes.c_uint32, u32p, ctypes.c_uint64, u32p, u32p, u32p]
     lib.csm_apply_batch.argtypes = [vp, ctypes.c_uint64, u32p, u32p, u32p, u8p, ctypes.POINTER(CsmBatchResult)]
     lib.csm_apply_batch_device.argtypes = [vp, ctypes.c_uint64, vp, vp, vp, vp, vp, ctypes.POINTER(CsmBatchResult)]
+    lib.csm_apply_batch_device_static.argtypes = [vp, ctypes.c_uint64, vp, vp, vp, vp, vp,
+                                                  ctypes.POINTER(CsmBatchResult)]
     lib.csm_get_edge_counts.argtypes = [vp, ctypes.c_int32, u64p, u64p, ctypes.c_uint32, u32p]
     lib.csm_get_embeddings.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(u32p), u64p]
     lib.csm_free.argtypes = [vp]
@@ -244,6 +246,15 @@ class Engine:
                                                     ctypes.c_void_p(lab_ptr),
                                                     ctypes.c_void_p(del_ptr) if del_ptr else None,
                                                     ctypes.c_void_p(stream) if stream else None, out))
+        return list(out)[: len(self.queries)]
+
+    def apply_device_static(self, n: int, src_ptr: int, dst_ptr: int, lab_ptr: int, del_ptr: Optional[int] = None,
+                            stream: Optional[int] = None) -> List[CsmBatchResult]:
+        """csm_apply_batch_device_static: the same batch, allocating nothing during the call."""
+        out = (CsmBatchResult * max(1, len(self.queries)))()
+        self._check(self.lib.csm_apply_batch_device_static(
+            self._h, n, ctypes.c_void_p(src_ptr), ctypes.c_void_p(dst_ptr), ctypes.c_void_p(lab_ptr),
+            ctypes.c_void_p(del_ptr) if del_ptr else None, ctypes.c_void_p(stream) if stream else None, out))
         return list(out)[: len(self.queries)]
 
     def edge_counts(self, qid: int):

@@ -5,12 +5,7 @@
 #include <new>
 #include <string>
 
-#include "engine.h"
-
-struct csm_engine {
-    csm::Engine impl;
-    explicit csm_engine(const csm_config &c) : impl(c) {}
-};
+#include "engine_handle.h"
 
 namespace {
 

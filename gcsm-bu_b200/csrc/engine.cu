@@ -344,6 +344,12 @@ csm_status Engine::load_graph(uint32_t nv, const uint32_t *vlabel, uint64_t ne, 
     CSM_CUDA(dalloc(&d_queue_, qcap_));
     CSM_CUDA(dalloc(&d_ready_, qcap_));
     CSM_CUDA(cudaMemset(d_ready_, 0, sizeof(uint32_t) * qcap_));
+    sc_.ctrl = d_ctrl_;
+    sc_.queue = d_queue_;
+    sc_.ready = d_ready_;
+    sc_.qcap = qcap_;
+    sc_.seed_lo = d_seed_lo_;
+    sc_.ticket_prefix = d_ticket_prefix_;
     const unsigned long long fbytes = cfg_.frontier_bytes ? cfg_.frontier_bytes : (1ull << 30);
     frontier_cap_ = std::max<unsigned long long>(1024, fbytes / 2 / sizeof(WorkItem));
     if (opt_.search_strategy >= 2) {
@@ -437,6 +443,27 @@ csm_status Engine::apply_device(uint64_t n, const uint32_t *src, const uint32_t 
     return run_batch(n, src, dst, elabel, is_delete, is_delete != nullptr, s, out);
 }
 
+csm_status Engine::apply_device_noalloc(uint64_t n, const uint32_t *src, const uint32_t *dst, const uint32_t *elabel,
+                                        const uint8_t *is_delete, cudaStream_t stream, const EnumScratch &scratch,
+                                        csm_batch_result *out) {
+    if (!graph_loaded_) return fail(CSM_ERR_STATE, "load the data graph first");
+    if (poisoned_) return fail(CSM_ERR_STATE, "the engine failed an earlier batch; recreate it");
+    if (n && (!src || !dst || !elabel)) return fail(CSM_ERR_INVALID_ARG, "null update array");
+    if (n > batch_cap_)
+        return fail(CSM_ERR_LIMIT, "batch of " + std::to_string(n) + " updates exceeds the " +
+                                       std::to_string(batch_cap_) +
+                                       " preallocated at load time (csm_config.max_batch); this call does not grow it");
+    cudaStream_t s = stream ? stream : stream_;
+    CSM_CUDA(cudaEventRecord(ev_[0], s));
+    const EnumScratch saved = sc_;
+    sc_ = scratch;
+    no_alloc_ = true;
+    const csm_status st = run_batch(n, src, dst, elabel, is_delete, is_delete != nullptr, s, out);
+    no_alloc_ = false;
+    sc_ = saved;
+    return st;
+}
+
 csm_status Engine::run_batch(uint64_t n, const uint32_t *src, const uint32_t *dst, const uint32_t *elabel,
                              const uint8_t *is_delete, bool has_delete, cudaStream_t s, csm_batch_result *out) {
     const uint32_t m = (uint32_t)(2 * n);
@@ -491,6 +518,11 @@ csm_status Engine::run_batch(uint64_t n, const uint32_t *src, const uint32_t *ds
         // The pool ran out during the merge, and the insertion phase skipped its work: lay the
         // lists out again in a larger pool, redo the merge (lists already merged are skipped),
         // the candidate refresh and the insertion phase.
+        if (no_alloc_) {
+            poisoned_ = true;
+            return fail(CSM_ERR_OOM, "adjacency pool exhausted in a call that may not allocate; size pool_entries "
+                                     "for the stream or apply batches through csm_apply_batch");
+        }
         stats_.pool_used = g_.pool_cap;
         csm_status cst = maybe_compact(s);
         if (cst != CSM_OK) return cst;
@@ -538,7 +570,7 @@ csm_status Engine::run_batch(uint64_t n, const uint32_t *src, const uint32_t *ds
         }
     }
     if (cfg_.materialize_rows) rows_valid_ = true;
-    return maybe_compact(s);
+    return no_alloc_ ? CSM_OK : maybe_compact(s);
 }
 
 csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
@@ -557,12 +589,12 @@ csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
     P.eff = bs_.eff;
     P.seg_flagged = phase == CSM_PHASE_INS ? bs_.seg_nins : bs_.seg_ndel;
     P.phase = phase;
-    P.seed_lo = d_seed_lo_;
-    P.ticket_prefix = d_ticket_prefix_;
-    P.queue = d_queue_;
-    P.ready = d_ready_;
-    P.qcap = qcap_;
-    P.ctrl = d_ctrl_;
+    P.seed_lo = sc_.seed_lo;
+    P.ticket_prefix = sc_.ticket_prefix;
+    P.queue = sc_.queue;
+    P.ready = sc_.ready;
+    P.qcap = sc_.qcap;
+    P.ctrl = sc_.ctrl;
     P.counts = d_counts_ + (phase == CSM_PHASE_INS ? np : 0);
     P.steal_min = cfg_.steal_chunk > 0 ? (uint32_t)cfg_.steal_chunk : 64u;
     // An idle warp leaves as soon as no warp holds work; the bound (about a minute of
@@ -578,8 +610,8 @@ csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
     phase_ran_[ph] = true;
     CSM_CUDA(cudaEventRecord(ev_[2 + 2 * ph], s));
 
-    launch_ctrl_reset(d_ctrl_, total_warps, ++epoch_, 0, s);
-    launch_seed_tickets(d_plans_, np, d_keys_, m, kl_, d_seed_lo_, d_ticket_prefix_, d_ctrl_, s);
+    launch_ctrl_reset(sc_.ctrl, total_warps, ++epoch_, 0, s);
+    launch_seed_tickets(d_plans_, np, d_keys_, m, kl_, sc_.seed_lo, sc_.ticket_prefix, sc_.ctrl, s);
     stats_.kernel_launches += 3;
     const WorkItem *frontier = nullptr;
     unsigned long long nfront = 0;
@@ -588,7 +620,7 @@ csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
         // frontier is small (strategy 2) or while it fits the budget (strategy 3); the size of
         // the next level is bounded from list sizes before it is written, so a level that would
         // not fit is never started and the search continues depth first from the current one.
-        CSM_CUDA(cudaMemcpyAsync(h_counts_ + 2 * np + 4, &d_ctrl_->nticket, sizeof(unsigned long long),
+        CSM_CUDA(cudaMemcpyAsync(h_counts_ + 2 * np + 4, &sc_.ctrl->nticket, sizeof(unsigned long long),
                                  cudaMemcpyDeviceToHost, s));
         CSM_CUDA(cudaStreamSynchronize(s));
         unsigned long long cur = h_counts_[2 * np + 4] * 32;  // seed candidates (upper bound)
@@ -601,9 +633,9 @@ csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
             if (frontier) {
                 h_counts_[2 * np + 4] = nfront;
                 CSM_CUDA(cudaMemcpyAsync(d_misc_, h_counts_ + 2 * np + 4, 8, cudaMemcpyHostToDevice, s));
-                CSM_CUDA(cudaMemsetAsync(&d_ctrl_->expand_bound, 0, 8, s));
+                CSM_CUDA(cudaMemsetAsync(&sc_.ctrl->expand_bound, 0, 8, s));
                 launch_expand_bound(P, frontier, d_misc_, s);
-                CSM_CUDA(cudaMemcpyAsync(h_counts_ + 2 * np + 5, &d_ctrl_->expand_bound, 8, cudaMemcpyDeviceToHost, s));
+                CSM_CUDA(cudaMemcpyAsync(h_counts_ + 2 * np + 5, &sc_.ctrl->expand_bound, 8, cudaMemcpyDeviceToHost, s));
                 CSM_CUDA(cudaStreamSynchronize(s));
                 bound = h_counts_[2 * np + 5];
             }
@@ -614,11 +646,11 @@ csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
             X.frontier = frontier;
             X.expand_out = d_frontier_[buf];
             X.expand_cap = frontier_cap_;
-            if (frontier) launch_ctrl_reset(d_ctrl_, total_warps, ++epoch_, nfront, s);
+            if (frontier) launch_ctrl_reset(sc_.ctrl, total_warps, ++epoch_, nfront, s);
             launch_enumerate(X, blocks_, warps_per_block_, s);
             stats_.enum_launches++;
             stats_.kernel_launches++;
-            CSM_CUDA(cudaMemcpyAsync(&h_ctrl_[ph], d_ctrl_, sizeof(EnumControl), cudaMemcpyDeviceToHost, s));
+            CSM_CUDA(cudaMemcpyAsync(&h_ctrl_[ph], sc_.ctrl, sizeof(EnumControl), cudaMemcpyDeviceToHost, s));
             CSM_CUDA(cudaStreamSynchronize(s));
             const unsigned long long rows_out = h_ctrl_[ph].out_rows;
             const unsigned int errb = h_ctrl_[ph].error;
@@ -636,7 +668,7 @@ csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
     D.donate = (strategy == 0 || strategy == 2) ? 1u : 0u;
     if (frontier) {
         D.frontier = frontier;
-        launch_ctrl_reset(d_ctrl_, total_warps, ++epoch_, nfront, s);
+        launch_ctrl_reset(sc_.ctrl, total_warps, ++epoch_, nfront, s);
         stats_.kernel_launches++;
     }
     launch_enumerate(D, blocks_, warps_per_block_, s);
@@ -644,7 +676,7 @@ csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
     stats_.kernel_launches++;
     CSM_CUDA(cudaEventRecord(ev_[3 + 2 * ph], s));
     // Statistics and error bits are read after the batch's final synchronisation.
-    CSM_CUDA(cudaMemcpyAsync(&h_ctrl_[ph], d_ctrl_, sizeof(EnumControl), cudaMemcpyDeviceToHost, s));
+    CSM_CUDA(cudaMemcpyAsync(&h_ctrl_[ph], sc_.ctrl, sizeof(EnumControl), cudaMemcpyDeviceToHost, s));
     if (rows) {
         // Collect rows per query for csm_get_embeddings (a validation path: synchronous).
         CSM_CUDA(cudaStreamSynchronize(s));

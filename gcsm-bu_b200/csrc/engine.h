@@ -18,6 +18,17 @@
 
 namespace csm {
 
+// Scratch of the enumeration kernel: control block, donation queue with its ready flags, and
+// the per-plan seed ranges and ticket prefixes (3 * nplans and nplans + 1 words).
+struct EnumScratch {
+    EnumControl *ctrl = nullptr;
+    WorkItem *queue = nullptr;
+    uint32_t *ready = nullptr;
+    uint32_t qcap = 0;
+    uint32_t *seed_lo = nullptr;
+    uint32_t *ticket_prefix = nullptr;
+};
+
 struct Options {
     Order order = Order::kGcsm;
     int search_strategy = 2;  // 0 DFS+stealing, 1 DFS, 2 dynamic BFS-DFS, 3 BFS
@@ -44,6 +55,15 @@ class Engine {
                           const uint8_t *is_delete, csm_batch_result *out);
     csm_status apply_device(uint64_t n, const uint32_t *src, const uint32_t *dst, const uint32_t *elabel,
                             const uint8_t *is_delete, cudaStream_t stream, csm_batch_result *out);
+    // The batch pipeline with caller-provided enumeration scratch and no allocation: batches
+    // beyond the preallocated capacity are rejected and the adjacency pool is never regrown.
+    csm_status apply_device_noalloc(uint64_t n, const uint32_t *src, const uint32_t *dst, const uint32_t *elabel,
+                                    const uint8_t *is_delete, cudaStream_t stream, const EnumScratch &scratch,
+                                    csm_batch_result *out);
+    uint32_t num_plans() const { return (uint32_t)plans_.size(); }
+    uint64_t batch_capacity() const { return batch_cap_; }
+    int device() const { return device_; }
+    cudaStream_t stream() const { return stream_; }
     csm_status edge_counts(int32_t qid, uint64_t *pos, uint64_t *neg, uint32_t capacity, uint32_t *n_out) const;
     csm_status embeddings(int32_t qid, int32_t sign, uint32_t **rows, uint64_t *nrows);
     csm_status describe(int32_t qid, char *buf, size_t n) const;
@@ -126,6 +146,8 @@ class Engine {
     EnumControl *h_ctrl_ = nullptr;           // pinned: control block of the DEL and INS launches
     unsigned long long *d_misc_ = nullptr;    // small device scratch
     bool phase_ran_[2] = {false, false};
+    EnumScratch sc_;                          // scratch used by enumerate_phase
+    bool no_alloc_ = false;                   // inside apply_device_noalloc
     int warps_per_block_ = 8;
     int blocks_ = 0;
 

@@ -154,6 +154,30 @@ csm_status csm_apply_batch_device(csm_engine *engine, uint64_t n, const uint32_t
                                   csm_batch_result *per_query_out);
 
 /*
+ * No counterpart in the reference.  csm_apply_batch_device for callers that cannot allocate
+ * device memory while they apply updates (processes that reserve their whole memory budget up
+ * front, hosts that own all device memory).  The call allocates nothing: the enumeration
+ * kernel's scratch lives in one array of CSM_STATIC_SCRATCH_BYTES compiled into the library,
+ * which every GPU that loads the library holds until the process exits.
+ *  - Limits: at most CSM_STATIC_MAX_PLANS query edges over all registered queries, and no
+ *    more updates than the batch capacity preallocated when the graph was loaded
+ *    (csm_config.max_batch); larger requests fail with CSM_ERR_LIMIT.  The adjacency pool is
+ *    never regrown: if a batch does not fit, the call fails with CSM_ERR_OOM (size
+ *    csm_config.pool_entries for the stream).
+ *  - The first call on a device looks up the array's device address; make that first call
+ *    before any stream capture.
+ *  - All calls on one device share the array, which keeps the last call's contents (the call
+ *    clears what must start at zero).  Calls that overlap on the GPU — other streams, other
+ *    engines, other threads — race on it: serialise them.
+ */
+#define CSM_STATIC_SCRATCH_BYTES (8u << 20)
+#define CSM_STATIC_MAX_PLANS 4096u
+csm_status csm_apply_batch_device_static(csm_engine *engine, uint64_t n, const uint32_t *d_src,
+                                         const uint32_t *d_dst, const uint32_t *d_elabel,
+                                         const uint8_t *d_is_delete, void *stream,
+                                         csm_batch_result *per_query_out);
+
+/*
  * Per-query-edge split of the last batch's counts, in the query's qe_list_ order
  * (graph.cpp:332-347): entry i counts the embeddings whose last query edge mapped to an
  * updated data edge is qe_list_[i] (the decomposition of technique_permutation.h:125-212).
