@@ -44,6 +44,7 @@ def parse():
     ap.add_argument("--config", default="c2")
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--nqueries", type=int, default=None)
+    ap.add_argument("--batch", type=int, default=None, help="override the configuration's batch size")
     ap.add_argument("--strategy", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-queries", type=int, default=10)
@@ -363,7 +364,9 @@ def main():
     args = parse()
     world, rank, local = dist_init(args)
     from csm import gen
-    cfg = gen.scaled(args.config, args.scale) if args.scale != 1.0 else None
+    cfg = gen.scaled(args.config, args.scale) if args.scale != 1.0 else dict(gen.CONFIGS[args.config])
+    if args.batch:
+        cfg["batch"] = args.batch
     w = gen.make_workload(args.config, cfg, nqueries=args.nqueries)
     if args.impl == "reference":
         run_reference(args, w, world, rank)
