@@ -351,7 +351,9 @@ def run_ours(args, w, world, rank, local):
                      "kernel": "k_enumerate",
                      "algorithmic_bytes_per_launch": alg_bytes / launches,
                      "avg_launch_ms": 1e3 * enum_s / launches,
-                     "traffic": traffic.get("dram_bytes_per_launch") if traffic else None},
+                     "traffic": (traffic["dram_bytes_per_algorithmic_byte"] * alg_bytes / launches) if traffic else None,
+                     "traffic_note": "DRAM bytes per launch scaled from the committed ncu capture "
+                                     "(profiles/enumerate_traffic.json) by algorithmic bytes" if traffic else None},
         "phase_ms_per_step": {"enumerate": 1e3 * enum_s / args.steps, "apply": 1e3 * apply_s / args.steps},
         "clocks": clk.summary(),
     }
