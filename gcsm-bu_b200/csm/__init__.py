@@ -59,7 +59,8 @@ class CsmConfig(ctypes.Structure):
         ("blocks_per_sm", ctypes.c_int32),
         ("warps_per_block", ctypes.c_int32),
         ("steal_chunk", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 5),
+        ("occupancy", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 4),
     ]
 
 

@@ -44,7 +44,7 @@ struct DevLevel {
     uint8_t nbn;                  // number of backward neighbours
     uint16_t old_mask;            // bit k: backward edge k must not be a batch edge
     uint8_t qv;                   // query vertex id
-    uint8_t pad0;
+    uint8_t bn_base;              // first slot of this level's lists in a flat per-plan array
     uint32_t nlf_bitmap;          // candidate bitmap (NLF filter) of this query vertex
     uint32_t pad1[2];
 };

@@ -84,7 +84,8 @@ csm_status Engine::init() {
     // Persistent launch: never more blocks than can be resident at once.  Warps that run out
     // of work wait for the others while any warp holds work, so a block that could only start
     // after resident blocks exit would stall the launch until the idle bound runs out.
-    const int resident = enum_blocks_per_sm(warps_per_block_);
+    occupancy_ = cfg_.occupancy >= 4 && cfg_.occupancy <= 6 ? cfg_.occupancy : 4;
+    const int resident = enum_blocks_per_sm(warps_per_block_, occupancy_);
     const int bps = cfg_.blocks_per_sm > 0 && cfg_.blocks_per_sm < resident ? cfg_.blocks_per_sm : resident;
     blocks_ = sm_count_ * bps;
     CSM_CUDA(dalloc(&d_ctrl_, 1));
@@ -647,7 +648,7 @@ csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
             X.expand_out = d_frontier_[buf];
             X.expand_cap = frontier_cap_;
             if (frontier) launch_ctrl_reset(sc_.ctrl, total_warps, ++epoch_, nfront, s);
-            launch_enumerate(X, blocks_, warps_per_block_, s);
+            launch_enumerate(X, blocks_, warps_per_block_, occupancy_, s);
             stats_.enum_launches++;
             stats_.kernel_launches++;
             CSM_CUDA(cudaMemcpyAsync(&h_ctrl_[ph], sc_.ctrl, sizeof(EnumControl), cudaMemcpyDeviceToHost, s));
@@ -671,7 +672,7 @@ csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
         launch_ctrl_reset(sc_.ctrl, total_warps, ++epoch_, nfront, s);
         stats_.kernel_launches++;
     }
-    launch_enumerate(D, blocks_, warps_per_block_, s);
+    launch_enumerate(D, blocks_, warps_per_block_, occupancy_, s);
     stats_.enum_launches++;
     stats_.kernel_launches++;
     CSM_CUDA(cudaEventRecord(ev_[3 + 2 * ph], s));

@@ -149,6 +149,7 @@ class Engine {
     EnumScratch sc_;                          // scratch used by enumerate_phase
     bool no_alloc_ = false;                   // inside apply_device_noalloc
     int warps_per_block_ = 8;
+    int occupancy_ = 4;                       // enumeration kernel variant (blocks per SM)
     int blocks_ = 0;
 
     // Results of the last batch.

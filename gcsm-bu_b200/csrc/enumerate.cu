@@ -39,9 +39,12 @@ struct __align__(16) WarpState {
     uint32_t lo[CSM_MAXQV];
     uint32_t hi[CSM_MAXQV];
     uint32_t base[CSM_MAXQV];
-    uint32_t poff[CSM_MAXQV][CSM_MAXBN];
-    uint32_t psz[CSM_MAXQV][CSM_MAXBN];
-    uint32_t cur[CSM_MAXQV][CSM_MAXBN];   // per probe list: entries before it are below the next chunk
+    // Backward-neighbour lists of every level, in one flat array: level d uses slots
+    // [lv[d].bn_base, lv[d].bn_base + nbn) (all levels together hold at most CSM_MAXQE lists).
+    uint32_t poff[CSM_MAXQE];
+    uint32_t psz[CSM_MAXQE];
+    uint32_t cur[CSM_MAXQE];   // per probe list: entries before it are below the next chunk
+    uint8_t bnb[CSM_MAXQV];
     uint32_t nlf[CSM_MAXQV];
     uint16_t oldm[CSM_MAXQV];
     uint8_t nbuf[CSM_MAXQV];
@@ -215,9 +218,10 @@ __device__ void enter_level(WarpState &S, const EnumParams &P, const DevPlan *pl
         const uint32_t dep = __ldg(&lv->bn_depth[lane]);
         const uint32_t v = S.f[dep];
         const uint2 ms = __ldg(P.g.meta + (size_t)rel * P.g.V + v);
-        S.poff[d][lane] = ms.x;
-        S.psz[d][lane] = ms.y;
-        S.cur[d][lane] = 0;
+        const uint32_t slot = __ldg(&lv->bn_base) + lane;
+        S.poff[slot] = ms.x;
+        S.psz[slot] = ms.y;
+        S.cur[slot] = 0;
         sz = ms.y;
     }
     const uint32_t piv = warp_min_index(sz, lane);
@@ -225,8 +229,10 @@ __device__ void enter_level(WarpState &S, const EnumParams &P, const DevPlan *pl
     if (lane == 0) {
         S.piv[d] = (uint8_t)piv;
         S.nbn[d] = (uint8_t)nbn;
-        S.base[d] = S.poff[d][piv];
-        const uint32_t psize = S.psz[d][piv];
+        const uint32_t bb = __ldg(&lv->bn_base);
+        S.bnb[d] = (uint8_t)bb;
+        S.base[d] = S.poff[bb + piv];
+        const uint32_t psize = S.psz[bb + piv];
         S.lo[d] = rlo;
         S.hi[d] = rhi < psize ? rhi : psize;
         S.nbuf[d] = 0;
@@ -631,9 +637,10 @@ __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, unsign
             for (uint32_t k = 0; k < nbn; k++) {
                 if (k == piv) continue;
                 if (!__any_sync(0xffffffffu, ok)) break;
-                const uint32_t *L = P.g.pool + S.poff[d][k];
-                const uint32_t c0 = S.cur[d][k];
-                const uint32_t hi = warp_lower_bound(L, c0, S.psz[d][k], (target + 1) << 1, lane);
+                const uint32_t slot = S.bnb[d] + k;
+                const uint32_t *L = P.g.pool + S.poff[slot];
+                const uint32_t c0 = S.cur[slot];
+                const uint32_t hi = warp_lower_bound(L, c0, S.psz[slot], (target + 1) << 1, lane);
                 const uint32_t W = hi - c0;
                 uint32_t e = 0xFFFFFFFFu;
                 if (W <= 32) {
@@ -648,7 +655,7 @@ __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, unsign
                     probes++;
                     ok = e != 0xFFFFFFFFu && !(((oldm >> k) & 1u) && (e & 1u));
                 }
-                if (lane == 0) S.cur[d][k] = hi;
+                if (lane == 0) S.cur[slot] = hi;
             }
         }
         __syncwarp();
@@ -728,7 +735,9 @@ __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, unsign
     return cnt;
 }
 
-__global__ void __launch_bounds__(256, 4) k_enumerate(EnumParams P) {
+// MINB resident blocks of 256 threads per SM: the register budget per thread follows from it.
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_enumerate(EnumParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
     WarpState &S = reinterpret_cast<WarpState *>(smem)[threadIdx.x >> 5];
     const uint32_t lane = lane_id();
@@ -884,19 +893,32 @@ __global__ void k_expand_bound(EnumParams P, const WorkItem *items, const unsign
 
 size_t enum_smem_bytes(int warps_per_block) { return sizeof(WarpState) * (size_t)warps_per_block; }
 
-int enum_blocks_per_sm(int warps_per_block) {
+namespace {
+using EnumKernel = void (*)(EnumParams);
+EnumKernel enum_kernel(int occupancy) {
+    switch (occupancy) {
+        case 4: return k_enumerate<4>;
+        case 6: return k_enumerate<6>;
+        case 5: return k_enumerate<5>;
+        default: return k_enumerate<4>;
+    }
+}
+}  // namespace
+
+int enum_blocks_per_sm(int warps_per_block, int occupancy) {
     const size_t smem = enum_smem_bytes(warps_per_block);
-    cudaFuncSetAttribute(k_enumerate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    EnumKernel k = enum_kernel(occupancy);
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_enumerate, warps_per_block * 32, smem) != cudaSuccess)
-        return 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, warps_per_block * 32, smem) != cudaSuccess) return 1;
     return nb > 0 ? nb : 1;
 }
 
-void launch_enumerate(const EnumParams &p, int blocks, int warps_per_block, cudaStream_t s) {
+void launch_enumerate(const EnumParams &p, int blocks, int warps_per_block, int occupancy, cudaStream_t s) {
     const size_t smem = enum_smem_bytes(warps_per_block);
-    cudaFuncSetAttribute(k_enumerate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_enumerate<<<blocks, warps_per_block * 32, smem, s>>>(p);
+    EnumKernel k = enum_kernel(occupancy);
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k<<<blocks, warps_per_block * 32, smem, s>>>(p);
 }
 
 void launch_seed_tickets(const DevPlan *plans, uint32_t nplans, const unsigned long long *keys, uint32_t m,

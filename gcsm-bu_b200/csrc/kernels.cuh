@@ -115,8 +115,10 @@ struct EnumParams {
 #define CSM_ENUM_MODE_EXPAND 2
 
 size_t enum_smem_bytes(int warps_per_block);
-int enum_blocks_per_sm(int warps_per_block);  // resident blocks per SM of the enumeration kernel
-void launch_enumerate(const EnumParams &p, int blocks, int warps_per_block, cudaStream_t s);
+// Resident blocks per SM of the enumeration kernel compiled for `occupancy` (4, 5 or 6)
+// resident 256-thread blocks per SM.
+int enum_blocks_per_sm(int warps_per_block, int occupancy);
+void launch_enumerate(const EnumParams &p, int blocks, int warps_per_block, int occupancy, cudaStream_t s);
 void launch_seed_tickets(const DevPlan *plans, uint32_t nplans, const unsigned long long *keys, uint32_t m,
                          KeyLayout kl, uint32_t *seed_lo, uint32_t *ticket_prefix, EnumControl *ctrl,
                          cudaStream_t s);

@@ -504,8 +504,11 @@ std::vector<HostPlan> build_plans(const Query &q, uint16_t query_id, uint32_t nl
         for (uint32_t d = 0; d < n; d++) dp.order[d] = order[d];
         dp.nlf0 = nlf_base + order[0];
         dp.nlf1 = nlf_base + order[1];
+        uint32_t bn_base = 0;
         for (uint32_t d = 0; d < n; d++) {
             DevLevel &lv = dp.lv[d];
+            lv.bn_base = (uint8_t)bn_base;
+            bn_base += (uint32_t)hp.bn[d].size();
             lv.qv = order[d];
             lv.nlf_bitmap = nlf_base + order[d];
             lv.nbn = (uint8_t)hp.bn[d].size();

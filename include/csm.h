@@ -71,7 +71,9 @@ typedef struct csm_config {
     int32_t blocks_per_sm;          /* persistent enumeration launch shape; 0 = automatic */
     int32_t warps_per_block;        /* 0 = automatic */
     int32_t steal_chunk;            /* minimum candidate range split by work donation; 0 = auto */
-    int32_t reserved[5];
+    int32_t occupancy;              /* enumeration kernel built for 4, 5 or 6 resident 256-thread
+                                       blocks per SM (fewer registers per thread); 0 = 4 */
+    int32_t reserved[4];
 } csm_config;
 
 /* Per-query result of one batch. */
