@@ -518,6 +518,110 @@ __device__ void write_row(const EnumParams &P, const DevPlan *pl, const WarpStat
     row[1 + pl->order[d]] = w;
 }
 
+// Last counting level with packed siblings.  The buffered candidates s_0..s_{k-1} of level
+// d = n - 2 each open a last level whose candidate lists are usually short, so instead of one
+// pass per sibling the warp scans all their pivot lists at once, one (sibling, position) pair
+// per lane.  A lane finds its sibling by a shuffle search over the inclusive prefix of list
+// lengths and checks its candidate like the per-sibling scan (flag rule, injectivity, NLF
+// bitmap, membership in the other backward lists by binary search).  Returns false (nothing
+// counted) when the lists are long enough for the per-sibling scan to fill the warp.
+__device__ bool count_last_packed(WarpState &S, const EnumParams &P, const DevPlan *pl, uint32_t d,
+                                  unsigned long long &cnt, unsigned long long &scans, unsigned long long &probes) {
+    const uint32_t lane = lane_id();
+    const uint32_t L = d + 1;
+    const DevLevel *lv = &pl->lv[L];
+    const uint32_t nbn = __ldg(&lv->nbn);
+    const uint32_t oldm = __ldg(&lv->old_mask);
+    const uint32_t *nlf = bitmap(P, __ldg(&lv->nlf_bitmap));
+    const uint32_t ps = S.pos[d], k = S.nbuf[d] - ps;
+    // Shared lists: backward neighbours matched before depth d (same for every sibling).
+    // sib_b = the backward neighbour at depth d (at most one), whose list is the sibling's own.
+    const uint32_t bb = __ldg(&lv->bn_base);
+    uint32_t sib_b = 0xFFu, sh_min = 0xFFFFFFFFu, sh_piv = 0;
+    for (uint32_t b = 0; b < nbn; b++) {
+        const uint32_t dep = __ldg(&lv->bn_depth[b]);
+        if (dep == d) {
+            sib_b = b;
+            continue;
+        }
+        const uint2 ms = __ldg(P.g.meta + (size_t)__ldg(&lv->bn_rel[b]) * P.g.V + S.f[dep]);
+        if (lane == 0) {
+            S.poff[bb + b] = ms.x;  // level L's own slots: it is counted, never entered
+            S.psz[bb + b] = ms.y;
+        }
+        if (ms.y < sh_min) {
+            sh_min = ms.y;
+            sh_piv = b;
+        }
+    }
+    __syncwarp();
+    // Per sibling (lane j < k): its own list, its pivot and the pivot's list.
+    uint32_t sv = 0, s_off = 0, s_sz = 0, pv = sh_piv, p_off = 0, p_len = 0;
+    if (lane < k) {
+        sv = S.buf[d][ps + lane];
+        if (sib_b != 0xFFu) {
+            const uint2 ms = __ldg(P.g.meta + (size_t)__ldg(&lv->bn_rel[sib_b]) * P.g.V + sv);
+            s_off = ms.x;
+            s_sz = ms.y;
+        }
+        if (sib_b != 0xFFu && s_sz <= sh_min) {
+            pv = sib_b;
+            p_off = s_off;
+            p_len = s_sz;
+        } else {
+            p_off = S.poff[bb + sh_piv];
+            p_len = sh_min;
+        }
+    }
+    // Inclusive prefix of pivot lengths.
+    uint32_t incl = p_len;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += t;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    if (total > 4u * k) return false;  // longer lists: the per-sibling scan fills the warp better
+    for (uint32_t g0 = 0; g0 < total; g0 += 32) {
+        const uint32_t g = g0 + lane;
+        // Sibling of position g: the first lane whose inclusive prefix exceeds g.
+        uint32_t j = 0;
+#pragma unroll
+        for (uint32_t step = 16; step > 0; step >>= 1)
+            if (__shfl_sync(0xffffffffu, incl, j + step - 1) <= g) j += step;
+        const uint32_t jc = j < 31 ? j : 31;
+        const uint32_t excl_j = __shfl_sync(0xffffffffu, incl, jc) - __shfl_sync(0xffffffffu, p_len, jc);
+        const uint32_t c_sv = __shfl_sync(0xffffffffu, sv, jc);
+        const uint32_t c_soff = __shfl_sync(0xffffffffu, s_off, jc);
+        const uint32_t c_ssz = __shfl_sync(0xffffffffu, s_sz, jc);
+        const uint32_t c_pv = __shfl_sync(0xffffffffu, pv, jc);
+        const uint32_t c_poff = __shfl_sync(0xffffffffu, p_off, jc);
+        bool ok = g < total;
+        uint32_t w = 0;
+        if (ok) {
+            const uint32_t e = __ldg(P.g.pool + c_poff + (g - excl_j));
+            w = e >> 1;
+            scans++;
+            ok = !(((oldm >> c_pv) & 1u) && (e & 1u)) && w != c_sv;
+        }
+        for (uint32_t t = 0; ok && t < d; t++) ok = S.f[t] != w;
+        const uint32_t nlf_word = ok ? __ldg(nlf + (w >> 5)) : 0u;
+        for (uint32_t b = 0; ok && b < nbn; b++) {
+            if (b == c_pv) continue;
+            const uint32_t *list = b == sib_b ? P.g.pool + c_soff : P.g.pool + S.poff[bb + b];
+            const uint32_t sz = b == sib_b ? c_ssz : S.psz[bb + b];
+            const uint32_t e = find_entry(list, sz, w);
+            probes++;
+            ok = e != 0xFFFFFFFFu && !(((oldm >> b) & 1u) && (e & 1u));
+        }
+        if (ok) ok = (nlf_word >> (w & 31)) & 1u;
+        cnt += __popc(__ballot_sync(0xffffffffu, ok));
+    }
+    __syncwarp();
+    if (lane == 0) S.pos[d] = S.nbuf[d];
+    __syncwarp();
+    return true;
+}
+
 // Runs one work item to completion.  Returns the number of matches counted.
 __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, unsigned long long &scans,
                                        unsigned long long &probes, unsigned long long &tails, unsigned int &err) {
@@ -578,6 +682,10 @@ __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, unsign
             if (granted && !try_donate(S, P, pl, L0, d) && lane == 0) atomicAdd(&P.ctrl->hungry, 1u);
         }
         if (S.pos[d] < S.nbuf[d]) {
+            // Siblings whose subtree is only the last level: count them together.
+            if (d + 2 == n && E == n && d >= 2 && P.mode == CSM_ENUM_MODE_COUNT &&
+                count_last_packed(S, P, pl, d, cnt, scans, probes))
+                continue;
             // Descend into the next buffered candidate.
             const uint32_t c = S.buf[d][S.pos[d]];
             __syncwarp();
@@ -627,29 +735,37 @@ __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, unsign
                 ok = !(((oldm >> piv) & 1u) && (e & 1u));
             }
             for (uint32_t k = 0; ok && k < d; k++) ok = S.f[k] != cand;
-            if (ok) ok = test_bit(bitmap(P, S.nlf[d]), cand);
+            // The NLF word is loaded now and tested after the probes, so its latency overlaps
+            // theirs (probes are warp-wide and do not depend on it).
+            const uint32_t nlf_word = ok ? __ldg(bitmap(P, S.nlf[d]) + (cand >> 5)) : 0u;
             // Membership in the other backward lists.  The chunk's candidates ascend, so each
-            // list keeps a cursor; the warp brackets the chunk's window in the list and, when
-            // the window fits in a warp, checks membership by shuffles over the window.
+            // list keeps a cursor.  The 32 entries at the cursor are read first: when they
+            // reach past the chunk's largest candidate, the window is in registers and
+            // shuffles find each candidate (one dependent read).  Otherwise a 32-ary warp search
+            // brackets the window and lanes search inside it.
             const uint32_t nbn = S.nbn[d];
             const uint32_t vmask = __ballot_sync(0xffffffffu, idx < S.hi[d]);
             const uint32_t target = __shfl_sync(0xffffffffu, cand, 31 - __clz(vmask));
+            const uint32_t key_hi = (target + 1) << 1;
             for (uint32_t k = 0; k < nbn; k++) {
                 if (k == piv) continue;
                 if (!__any_sync(0xffffffffu, ok)) break;
                 const uint32_t slot = S.bnb[d] + k;
                 const uint32_t *L = P.g.pool + S.poff[slot];
                 const uint32_t c0 = S.cur[slot];
-                const uint32_t hi = warp_lower_bound(L, c0, S.psz[slot], (target + 1) << 1, lane);
-                const uint32_t W = hi - c0;
-                uint32_t e = 0xFFFFFFFFu;
-                if (W <= 32) {
-                    const uint32_t win = lane < W ? __ldg(L + c0 + lane) : 0xFFFFFFFFu;
+                const uint32_t size = S.psz[slot];
+                uint32_t win = c0 + lane < size ? __ldg(L + c0 + lane) : 0xFFFFFFFFu;
+                const uint32_t below = __ballot_sync(0xffffffffu, win < key_hi);
+                uint32_t e = 0xFFFFFFFFu, hi;
+                if (below != 0xffffffffu) {
+                    // The window [c0, hi) fits in the 32 entries just read.
+                    hi = c0 + __popc(below);
                     const uint32_t pos = shfl_lower_bound(win, cand << 1);
                     const uint32_t got = __shfl_sync(0xffffffffu, win, pos);
                     if ((got >> 1) == cand && got != 0xFFFFFFFFu) e = got;
-                } else if (ok) {
-                    e = find_entry(L + c0, W, cand);
+                } else {
+                    hi = warp_lower_bound(L, c0 + 32, size, key_hi, lane);
+                    if (ok) e = find_entry(L + c0, hi - c0, cand);
                 }
                 if (ok) {
                     probes++;
@@ -657,6 +773,7 @@ __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, unsign
                 }
                 if (lane == 0) S.cur[slot] = hi;
             }
+            if (ok) ok = (nlf_word >> (cand & 31)) & 1u;
         }
         __syncwarp();
         if (lane == 0) S.lo[d] += 32u;
