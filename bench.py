@@ -48,6 +48,16 @@ def parse():
     ap.add_argument("--strategy", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-queries", type=int, default=10)
+    ap.add_argument("--form", default="plain", choices=["plain", "batched", "served"],
+                    help="plain: one engine per standing query, a step is one batch for one query; "
+                         "batched: one engine for all standing queries, a step is one batch for all of them")
+    ap.add_argument("--autotune", type=int, default=0, help="batched form: batches the engine tunes its launch on")
+    ap.add_argument("--tenants", type=int, default=4, help="served form: query groups, one graph replica each")
+    ap.add_argument("--slots", type=int, default=4, help="served form: concurrent work units")
+    ap.add_argument("--rate", type=float, default=50.0, help="served form: Poisson arrival rate (batches/s)")
+    ap.add_argument("--budget-gb", type=float, default=80.0, help="served form: frontier memory budget")
+    ap.add_argument("--plain-steps", type=int, default=None,
+                    help="batched form: batches the plain path is timed on for the comparison (default: --steps)")
     return ap.parse_args()
 
 
@@ -362,6 +372,332 @@ def run_ours(args, w, world, rank, local):
     print(json.dumps(out))
 
 
+def device_arrays(b, dev):
+    import torch
+    dl = b.is_delete if b.is_delete is not None else np.zeros(len(b.src), dtype=np.uint8)
+    return tuple(torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+                 for a in (b.src.astype(np.int32), b.dst.astype(np.int32), b.elabels.astype(np.int32),
+                           dl.astype(np.uint8)))
+
+
+def pinned_batch(b):
+    import torch
+
+    import csm
+    arrs = []
+    for a in (b.src, b.dst, b.elabels):
+        h = torch.empty(len(a), dtype=torch.int32, pin_memory=True)
+        h.numpy()[:] = a.view(np.int32)
+        arrs.append(h)
+    dl = b.is_delete if b.is_delete is not None else np.zeros(len(b.src), dtype=np.uint8)
+    h = torch.empty(len(dl), dtype=torch.uint8, pin_memory=True)
+    h.numpy()[:] = dl
+    arrs.append(h)
+    return arrs, csm.Batch(arrs[0].numpy().view(np.uint32), arrs[1].numpy().view(np.uint32),
+                           arrs[2].numpy().view(np.uint32), arrs[3].numpy())
+
+
+def run_batched(args, w, world, rank, local):
+    """Batched form: one engine holds every standing query; a step applies one update batch and
+    counts the incremental matches of all queries in one launch per phase.  The plain path (one
+    engine per query, as `run_ours`) is timed on the same batches for the comparison, and the
+    per-query counts of both forms are compared batch by batch."""
+    import torch
+
+    import csm
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    tune = min(args.autotune, args.warmup)
+    eng = csm.Engine(device=local, algorithm=0, search_strategy=args.strategy, max_batch=w.batch_size,
+                     autotune_batches=tune)
+    for q in w.queries:
+        eng.load_query(q)
+    eng.load_graph(w.data)
+    seq = step_batches(w, args.warmup + 2 * args.steps)
+    warm, timed, timed_e2e = seq[: args.warmup], seq[args.warmup: args.warmup + args.steps], seq[args.warmup + args.steps:]
+    dev_cache = {}
+    for b in seq:
+        if id(b) not in dev_cache:
+            dev_cache[id(b)] = device_arrays(b, dev)
+
+    def apply_dev(e, b):
+        s, d, l, dl = dev_cache[id(b)]
+        return e.apply_device(len(b.src), s.data_ptr(), d.data_ptr(), l.data_ptr(), dl.data_ptr(), stream.cuda_stream)
+
+    for b in warm:
+        apply_dev(eng, b)
+    torch.cuda.synchronize(dev)
+    eng.reset_stats()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    matches, upd, lat, per_batch = 0, 0, [], []
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for b in timed:
+            res = apply_dev(eng, b)
+            per_batch.append([(r.positive, r.negative) for r in res])
+            matches += sum(r.positive + r.negative for r in res)
+            upd += len(b.src)
+            lat.append(res[0].latency_ns / 1e6)
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+    barrier(world)
+    t = ev0.elapsed_time(ev1) / 1e3
+    tmax = max_over_ranks(t, world, dev)
+    st = eng.stats()
+
+    pinned = {}
+    for b in timed_e2e:
+        if id(b) not in pinned:
+            pinned[id(b)] = pinned_batch(b)
+    matches_e2e, h2d = 0, 0
+    barrier(world)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for b in timed_e2e:
+        res = eng.apply(pinned[id(b)][1])
+        matches_e2e += sum(r.positive + r.negative for r in res)
+        h2d += 13 * len(b.src)
+    t_e2e = time.perf_counter() - t0
+    t_e2e_max = max_over_ranks(t_e2e, world, dev)
+    pool_mb = st.pool_capacity * 4 / 2 ** 20
+    eng.close()
+
+    # The plain path on the same batches: one engine per query, each batch applied to each.
+    nplain = args.steps if args.plain_steps is None else min(args.plain_steps, args.steps)
+    plain_t, plain_matches, identical = 0.0, 0, True
+    for qi, q in enumerate(w.queries):
+        e = csm.Engine(device=local, algorithm=0, search_strategy=args.strategy, max_batch=w.batch_size)
+        e.load_query(q)
+        e.load_graph(w.data)
+        for b in warm:
+            apply_dev(e, b)
+        torch.cuda.synchronize(dev)
+        ev0.record(stream)
+        got = []
+        for b in timed[:nplain]:
+            r = apply_dev(e, b)[0]
+            got.append((r.positive, r.negative))
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        plain_t += ev0.elapsed_time(ev1) / 1e3
+        plain_matches += sum(p + n for p, n in got)
+        identical &= all(got[i] == per_batch[i][qi] for i in range(nplain))
+        e.close()
+    plain_tmax = max_over_ranks(plain_t, world, dev)
+    if rank != 0:
+        return
+    batched_first = sum(sum(p + n for p, n in row) for row in per_batch[:nplain])
+    t_first = t * nplain / len(timed)
+    peak, peak_kind = measured_peaks()
+    enum_s = st.enum_ns / 1e9
+    launches = max(1, st.enum_launches)
+    alg_bytes = 4.0 * (st.enum_scan_entries + st.enum_probes + st.enum_tail_lists)
+    achieved = alg_bytes / enum_s / 1e9 if enum_s > 0 else 0.0
+    traffic = profile_traffic()
+    out = {
+        "metric": "incremental matches/sec", "value": world * matches / tmax, "unit": "matches/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tmax / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "form": "batched",
+        "config": {"workload": f"{w.name}: Chung-Lu {len(w.data.vlabels)} vertices, {len(w.data.src)} initial edges;"
+                               f" step = one {w.batch_size}-update batch for all {len(w.queries)} standing"
+                               " queries in one engine (stream, then its inverse)",
+                   "batch_size": w.batch_size, "queries": len(w.queries), "search_strategy": args.strategy,
+                   "autotune_batches": tune, "parallelism": f"replicas x{world}",
+                   "l2": f"inputs larger than L2 (adjacency pool {pool_mb:.0f} MiB, 126 MB L2)"},
+        "tuned": {"strategy": st.tuned_strategy, "steal_chunk": st.tuned_steal_chunk,
+                  "warps_per_block": st.tuned_warps_per_block, "occupancy": st.tuned_occupancy},
+        "update_edges_per_s": world * upd / tmax,
+        "p50_batch_ms": float(np.percentile(lat, 50)), "p99_batch_ms": float(np.percentile(lat, 99)),
+        "matches_per_step": matches / args.steps,
+        "plain": {"value": plain_matches / plain_tmax if plain_tmax else None, "unit": "matches/s",
+                  "steps": nplain, "ms_per_step": 1e3 * plain_tmax / max(1, nplain),
+                  "note": "one engine per query, each of the first steps' batches applied to each"},
+        "speedup_vs_plain": (batched_first / t_first) / (plain_matches / plain_tmax) if plain_matches and t_first else None,
+        "counts_identical_to_plain": bool(identical),
+        "e2e": {"value": world * matches_e2e / t_e2e_max, "unit": "matches/s",
+                "h2d_bytes_per_step": h2d // max(1, len(timed_e2e)), "d2h_bytes_per_step": 64 * len(w.queries)},
+        "gpu_launches": int(st.kernel_launches),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": f"{peak_kind} hbm_gbs", "kernel": "k_enumerate",
+                     "algorithmic_bytes_per_launch": alg_bytes / launches,
+                     "avg_launch_ms": 1e3 * enum_s / launches,
+                     "traffic": (traffic["dram_bytes_per_algorithmic_byte"] * alg_bytes / launches) if traffic else None},
+        "phase_ms_per_step": {"enumerate": 1e3 * enum_s / args.steps, "apply": 1e3 * st.apply_ns / 1e9 / args.steps},
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(out))
+
+
+def split_queries(queries, groups):
+    """Query indices in `groups` groups of similar total size (largest first, to the lightest)."""
+    order = sorted(range(len(queries)), key=lambda i: -len(queries[i].src))
+    out, load = [[] for _ in range(groups)], [0] * groups
+    for i in order:
+        g = min(range(groups), key=lambda k: load[k])
+        out[g].append(i)
+        load[g] += len(queries[i].src)
+    return [sorted(g) for g in out if g]
+
+
+def run_served(args, w, world, rank, local):
+    """Served form: the standing queries are split into tenants (each an engine over its own
+    replica of the data graph holding a group of queries) behind the serving loop of
+    csm_server.h.  Requests are the stream's batches, each for every tenant.  Phase 1 offers
+    them as a Poisson process at --rate batches/s and records the latency of each request from
+    its arrival to its counts (queueing included); phase 2 submits the next batches at once
+    and measures the sustained throughput (the line's value).  The plain path (one engine per
+    query, one batch at a time) is timed on the phase-2 batches for the comparison, and every
+    per-query count of both forms is compared."""
+    import torch
+
+    import csm
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream(dev)
+    groups = split_queries(w.queries, max(1, min(args.tenants, len(w.queries))))
+    engines = []
+    for g in groups:
+        e = csm.Engine(device=local, algorithm=0, search_strategy=args.strategy, max_batch=w.batch_size,
+                       frontier_bytes=1 << 20)
+        for qi in g:
+            e.load_query(w.queries[qi])
+        e.load_graph(w.data)
+        engines.append(e)
+    budget = int(args.budget_gb * (1 << 30))
+    srv = csm.Server(device=local, slots=args.slots, memory_budget=budget)
+    for e in engines:
+        srv.add_tenant(e)
+    seq = step_batches(w, args.warmup + 2 * args.steps)
+    warm, poisson, burst = seq[: args.warmup], seq[args.warmup: args.warmup + args.steps], seq[args.warmup + args.steps:]
+
+    def collect(ids):
+        rows, infos = [], []
+        for rid in ids:
+            info, res = srv.wait(rid)
+            if info.status != 0:
+                raise RuntimeError(f"request failed with status {info.status}")
+            per_q = [None] * len(w.queries)
+            at = 0
+            for g in groups:
+                for qi in g:
+                    per_q[qi] = (res[at].positive, res[at].negative)
+                    at += 1
+            rows.append(per_q)
+            infos.append(info)
+        return rows, infos
+
+    collect([srv.submit(b) for b in warm])
+    rng = np.random.default_rng(4242)
+    gaps = rng.exponential(1.0 / args.rate, size=len(poisson))
+    barrier(world)
+    with ClockSampler(local) as clk:
+        t0 = time.perf_counter()
+        ids, due = [], 0.0
+        for b, gap in zip(poisson, gaps):
+            due += gap
+            while time.perf_counter() - t0 < due:
+                time.sleep(min(0.001, max(0.0, due - (time.perf_counter() - t0))))
+            ids.append(srv.submit(b))
+        rows_p, infos_p = collect(ids)
+        span_p = (max(i.done_ns for i in infos_p) - min(i.arrival_ns for i in infos_p)) / 1e9
+        ids = [srv.submit(b) for b in burst]
+        rows_b, infos_b = collect(ids)
+        span_b = (max(i.done_ns for i in infos_b) - min(i.arrival_ns for i in infos_b)) / 1e9
+    barrier(world)
+    span_b_max = max_over_ranks(span_b, world, dev)
+    lat = [(i.done_ns - i.arrival_ns) / 1e6 for i in infos_p]
+    lat_b = [(i.done_ns - i.arrival_ns) / 1e6 for i in infos_b]
+    matches_p = sum(p + n for row in rows_p for p, n in row)
+    matches_b = sum(p + n for row in rows_b for p, n in row)
+    sst = srv.stats()
+    srv.close()
+    sts = [e.stats() for e in engines]
+    for e in engines:
+        e.close()
+
+    # The plain path on the phase-2 batches: one engine per query from the same graph state.
+    dev_cache = {}
+    for b in burst:
+        if id(b) not in dev_cache:
+            dev_cache[id(b)] = device_arrays(b, dev)
+    nplain = len(burst) if args.plain_steps is None else min(args.plain_steps, len(burst))
+    plain_t, plain_matches, identical = 0.0, 0, True
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for qi, q in enumerate(w.queries):
+        e = csm.Engine(device=local, algorithm=0, search_strategy=args.strategy, max_batch=w.batch_size)
+        e.load_query(q)
+        e.load_graph(w.data)
+        for b in warm + poisson:
+            e.apply(b)
+        torch.cuda.synchronize(dev)
+        ev0.record(stream)
+        got = []
+        for b in burst[:nplain]:
+            sd, dd, ld, dl = dev_cache[id(b)]
+            r = e.apply_device(len(b.src), sd.data_ptr(), dd.data_ptr(), ld.data_ptr(), dl.data_ptr(),
+                               stream.cuda_stream)[0]
+            got.append((r.positive, r.negative))
+        ev1.record(stream)
+        torch.cuda.synchronize(dev)
+        plain_t += ev0.elapsed_time(ev1) / 1e3
+        plain_matches += sum(p + n for p, n in got)
+        identical &= all(got[i] == rows_b[i][qi] for i in range(nplain))
+        e.close()
+    plain_tmax = max_over_ranks(plain_t, world, dev)
+    if rank != 0:
+        return
+    served_first = sum(p + n for row in rows_b[:nplain] for p, n in row)
+    served_first_t = (max(i.done_ns for i in infos_b[:nplain]) - min(i.arrival_ns for i in infos_b[:nplain])) / 1e9
+    peak, peak_kind = measured_peaks()
+    enum_s = sum(st.enum_ns for st in sts) / 1e9
+    launches = max(1, sum(st.enum_launches for st in sts))
+    alg_bytes = 4.0 * sum(st.enum_scan_entries + st.enum_probes + st.enum_tail_lists for st in sts)
+    achieved = alg_bytes / enum_s / 1e9 if enum_s > 0 else 0.0
+    h2d = 13 * sum(len(b.src) for b in burst) * len(groups) // max(1, len(burst))
+    sizes = [len(b.src) for b in w.batches]
+    out = {
+        "metric": "incremental matches/sec", "value": world * matches_b / span_b_max, "unit": "matches/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * span_b_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "form": "served",
+        "config": {"workload": f"{w.name}: Chung-Lu {len(w.data.vlabels)} vertices, {len(w.data.src)} initial edges;"
+                               f" {len(w.queries)} standing queries in {len(groups)} tenants (graph replicas);"
+                               f" requests = stream batches of {min(sizes)}..{max(sizes)} updates (stream, then"
+                               " its inverse), each for every tenant",
+                   "tenants": len(groups), "slots": args.slots, "memory_budget_gb": args.budget_gb,
+                   "search_strategy": args.strategy, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (20M-edge graph replicas, 126 MB L2)"},
+        "poisson": {"rate_per_s": args.rate, "requests": len(infos_p),
+                    "p50_latency_ms": float(np.percentile(lat, 50)), "p99_latency_ms": float(np.percentile(lat, 99)),
+                    "matches_per_s": matches_p / span_p if span_p else None,
+                    "update_edges_per_s": sum(len(b.src) for b in poisson) / span_p if span_p else None},
+        "p50_batch_ms": float(np.percentile(lat, 50)), "p99_batch_ms": float(np.percentile(lat, 99)),
+        "burst_p50_ms": float(np.percentile(lat_b, 50)), "burst_p99_ms": float(np.percentile(lat_b, 99)),
+        "update_edges_per_s": world * sum(len(b.src) for b in burst) / span_b_max,
+        "server": {"units": sst.units, "units_depth_first": sst.units_depth_first, "units_shrunk": sst.units_shrunk,
+                   "memory_waits": sst.memory_waits, "peak_frontier_mb": sst.peak_frontier_bytes / 2 ** 20,
+                   "peak_inflight": sst.peak_inflight},
+        "plain": {"value": plain_matches / plain_tmax if plain_tmax else None, "unit": "matches/s", "steps": nplain,
+                  "note": "one engine per query, each batch applied to each, device-resident updates"},
+        "speedup_vs_plain": (served_first / served_first_t) / (plain_matches / plain_tmax)
+        if plain_matches and served_first_t else None,
+        "counts_identical_to_plain": bool(identical),
+        "e2e": {"value": world * matches_b / span_b_max, "unit": "matches/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": 64 * len(w.queries),
+                "note": "requests carry host arrays; the span runs from the first arrival to the last counts on the host"},
+        "gpu_launches": int(sum(st.kernel_launches for st in sts)),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": f"{peak_kind} hbm_gbs", "kernel": "k_enumerate",
+                     "note": "enumeration time summed over tenants; overlapping units make this a lower bound"},
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(out))
+
+
 def main():
     args = parse()
     world, rank, local = dist_init(args)
@@ -372,6 +708,10 @@ def main():
     w = gen.make_workload(args.config, cfg, nqueries=args.nqueries)
     if args.impl == "reference":
         run_reference(args, w, world, rank)
+    elif args.form == "batched":
+        run_batched(args, w, world, rank, local)
+    elif args.form == "served":
+        run_served(args, w, world, rank, local)
     else:
         run_ours(args, w, world, rank, local)
     if world > 1:

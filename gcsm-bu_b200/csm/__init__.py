@@ -41,6 +41,12 @@ EXPORTED = [
     "csm_last_error", "csm_version",
 ]
 
+# Every symbol declared in include/csm_server.h.
+SERVER_EXPORTED = [
+    "csm_server_default_config", "csm_server_create", "csm_server_add_tenant", "csm_server_submit",
+    "csm_server_wait", "csm_server_get_stats", "csm_server_destroy", "csm_server_last_error",
+]
+
 
 class CsmConfig(ctypes.Structure):
     _fields_ = [
@@ -60,7 +66,8 @@ class CsmConfig(ctypes.Structure):
         ("warps_per_block", ctypes.c_int32),
         ("steal_chunk", ctypes.c_int32),
         ("occupancy", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 4),
+        ("autotune_batches", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 3),
     ]
 
 
@@ -81,7 +88,7 @@ class CsmStats(ctypes.Structure):
     _fields_ = [(name, ctypes.c_uint64) for name in (
         "batches", "enum_launches", "kernel_launches", "enum_scan_entries", "enum_probes",
         "enum_tail_lists", "donations", "enum_ns", "apply_ns", "pool_used", "pool_capacity",
-        "compactions")] + [("reserved", ctypes.c_uint64 * 4)]
+        "compactions", "tuned_strategy", "tuned_steal_chunk", "tuned_warps_per_block", "tuned_occupancy")]
 
 
 class CsmError(RuntimeError):
@@ -91,6 +98,29 @@ class CsmError(RuntimeError):
 
 
 _lib = None
+
+
+class CsmServerConfig(ctypes.Structure):
+    _fields_ = [
+        ("device", ctypes.c_int32),
+        ("slots", ctypes.c_int32),
+        ("memory_budget", ctypes.c_uint64),
+        ("min_frontier_bytes", ctypes.c_uint64),
+        ("max_pending", ctypes.c_uint32),
+        ("reserved", ctypes.c_int32 * 7),
+    ]
+
+
+class CsmRequestInfo(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int32), ("nresults", ctypes.c_uint32)] + [
+        (n, ctypes.c_uint64) for n in ("arrival_ns", "start_ns", "done_ns", "frontier_bytes", "device_ns")] + [
+        ("reserved", ctypes.c_uint64 * 2)]
+
+
+class CsmServerStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in (
+        "requests", "units", "units_depth_first", "units_shrunk", "memory_waits", "peak_frontier_bytes",
+        "peak_inflight")] + [("reserved", ctypes.c_uint64 * 5)]
 
 
 def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
@@ -124,7 +154,16 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.csm_reset_stats.argtypes = [vp]
     lib.csm_device_memory.argtypes = [vp, u64p, u64p]
     lib.csm_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
-    for name in EXPORTED:
+    lib.csm_server_default_config.argtypes = [ctypes.POINTER(CsmServerConfig)]
+    lib.csm_server_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(CsmServerConfig)]
+    lib.csm_server_add_tenant.argtypes = [vp, vp, ctypes.POINTER(ctypes.c_int32)]
+    lib.csm_server_submit.argtypes = [vp, ctypes.c_int32, ctypes.c_uint64, u32p, u32p, u32p, u8p, u64p]
+    lib.csm_server_wait.argtypes = [vp, ctypes.c_uint64, ctypes.c_int64, ctypes.POINTER(CsmRequestInfo),
+                                    ctypes.POINTER(CsmBatchResult), ctypes.c_uint32]
+    lib.csm_server_get_stats.argtypes = [vp, ctypes.POINTER(CsmServerStats)]
+    lib.csm_server_destroy.argtypes = [vp]
+    lib.csm_server_last_error.argtypes = [vp, ctypes.c_char_p, ctypes.c_size_t]
+    for name in EXPORTED + SERVER_EXPORTED:
         if name != "csm_version":
             getattr(lib, name).restype = ctypes.c_int32
     _lib = lib
@@ -290,6 +329,87 @@ class Engine:
 
     def reset_stats(self):
         self._check(self.lib.csm_reset_stats(self._h))
+
+
+class Server:
+    """Continuous-batching serving loop (include/csm_server.h): tenant engines on one GPU, work
+    units admitted to slots as slots and frontier memory free up."""
+
+    def __init__(self, device: int = 0, slots: int = 4, memory_budget: int = 8 << 30,
+                 min_frontier_bytes: int = 16 << 20, max_pending: int = 4096):
+        self.lib = load_library()
+        cfg = CsmServerConfig()
+        self.lib.csm_server_default_config(ctypes.byref(cfg))
+        cfg.device, cfg.slots, cfg.memory_budget = device, slots, memory_budget
+        cfg.min_frontier_bytes, cfg.max_pending = min_frontier_bytes, max_pending
+        self._h = ctypes.c_void_p()
+        rc = self.lib.csm_server_create(ctypes.byref(self._h), ctypes.byref(cfg))
+        if rc != CSM_OK:
+            raise CsmError(rc, self._err(None))
+        self.tenants: List[Engine] = []
+        self._nres = {}
+
+    def _err(self, h) -> str:
+        buf = ctypes.create_string_buffer(1024)
+        self.lib.csm_server_last_error(h, buf, len(buf))
+        return buf.value.decode(errors="replace")
+
+    def _check(self, rc: int):
+        if rc != CSM_OK:
+            raise CsmError(rc, self._err(self._h))
+
+    def add_tenant(self, eng: Engine) -> int:
+        tid = ctypes.c_int32(-1)
+        self._check(self.lib.csm_server_add_tenant(self._h, eng._h, ctypes.byref(tid)))
+        self.tenants.append(eng)
+        return tid.value
+
+    def submit(self, b: Batch, tenant: int = -1) -> int:
+        s, d, l = _u32(b.src), _u32(b.dst), _u32(b.elabels)
+        dp = None
+        if b.is_delete is not None:
+            dl = np.ascontiguousarray(np.asarray(b.is_delete, dtype=np.uint8))
+            dp = _ptr(dl, ctypes.c_uint8)
+        rid = ctypes.c_uint64()
+        self._check(self.lib.csm_server_submit(self._h, tenant, len(s), _ptr(s), _ptr(d), _ptr(l), dp,
+                                               ctypes.byref(rid)))
+        ts = self.tenants if tenant < 0 else [self.tenants[tenant]]
+        self._nres[rid.value] = sum(len(t.queries) for t in ts)
+        return rid.value
+
+    def wait(self, rid: int, timeout_ms: int = -1):
+        """Returns (info, per-query results), or None if the request is still running."""
+        n = self._nres[rid]
+        out = (CsmBatchResult * max(1, n))()
+        info = CsmRequestInfo()
+        rc = self.lib.csm_server_wait(self._h, rid, timeout_ms, ctypes.byref(info), out, n)
+        if rc == -4:
+            return None
+        del self._nres[rid]
+        self._check(rc)
+        return info, list(out)[:n]
+
+    def stats(self) -> CsmServerStats:
+        st = CsmServerStats()
+        self._check(self.lib.csm_server_get_stats(self._h, ctypes.byref(st)))
+        return st
+
+    def close(self):
+        if self._h:
+            self.lib.csm_server_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def version() -> str:

@@ -68,6 +68,22 @@ csm_status Engine::cuda_fail(cudaError_t e, const char *where) {
         if (e__ != cudaSuccess) return cuda_fail(e__, #call); \
     } while (0)
 
+void Engine::set_launch_config(const LaunchConfig &c) {
+    // Persistent launch: never more blocks than can be resident at once.  Warps that run out
+    // of work wait for the others while any warp holds work, so a block that could only start
+    // after resident blocks exit would stall the launch until the idle bound runs out.
+    lc_ = c;
+    warps_per_block_ = c.warps_per_block;
+    occupancy_ = c.occupancy;
+    const int resident = enum_blocks_per_sm(warps_per_block_, occupancy_);
+    const int bps = cfg_.blocks_per_sm > 0 && cfg_.blocks_per_sm < resident ? cfg_.blocks_per_sm : resident;
+    blocks_ = sm_count_ * bps;
+    stats_.tuned_strategy = (uint64_t)c.strategy;
+    stats_.tuned_steal_chunk = c.steal_chunk;
+    stats_.tuned_warps_per_block = (uint64_t)c.warps_per_block;
+    stats_.tuned_occupancy = (uint64_t)c.occupancy;
+}
+
 csm_status Engine::init() {
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(CSM_ERR_NO_DEVICE, "no CUDA device");
@@ -81,13 +97,38 @@ csm_status Engine::init() {
     CSM_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     for (auto &e : ev_) CSM_CUDA(cudaEventCreate(&e));
     warps_per_block_ = cfg_.warps_per_block > 0 && cfg_.warps_per_block <= 8 ? cfg_.warps_per_block : 8;
-    // Persistent launch: never more blocks than can be resident at once.  Warps that run out
-    // of work wait for the others while any warp holds work, so a block that could only start
-    // after resident blocks exit would stall the launch until the idle bound runs out.
-    occupancy_ = cfg_.occupancy >= 4 && cfg_.occupancy <= 6 ? cfg_.occupancy : 4;
-    const int resident = enum_blocks_per_sm(warps_per_block_, occupancy_);
-    const int bps = cfg_.blocks_per_sm > 0 && cfg_.blocks_per_sm < resident ? cfg_.blocks_per_sm : resident;
-    blocks_ = sm_count_ * bps;
+    LaunchConfig lc;
+    lc.strategy = opt_.search_strategy;
+    lc.steal_chunk = cfg_.steal_chunk > 0 ? (uint32_t)cfg_.steal_chunk : 64u;
+    lc.warps_per_block = warps_per_block_;
+    lc.occupancy = cfg_.occupancy >= 4 && cfg_.occupancy <= 6 ? cfg_.occupancy : 4;
+    lc.frontier_mult = 8;
+    set_launch_config(lc);
+    if (cfg_.autotune_batches > 0) {
+        // Candidates: the configured one first, then variations of one knob each.
+        tune_cands_.push_back(lc);
+        auto add = [&](LaunchConfig c) { tune_cands_.push_back(c); };
+        LaunchConfig c = lc;
+        c.strategy = lc.strategy == 0 ? 2 : 0;
+        add(c);
+        c = lc;
+        c.steal_chunk = 256;
+        add(c);
+        c = lc;
+        c.warps_per_block = 4;
+        add(c);
+        c = lc;
+        c.occupancy = 5;
+        add(c);
+        if (lc.strategy >= 2) {
+            c = lc;
+            c.frontier_mult = 64;
+            add(c);
+        }
+        tune_ms_.assign(tune_cands_.size(), 0.0);
+        tune_left_ = cfg_.autotune_batches;
+        for (size_t i = 0; i < 2 * tune_cands_.size(); i++) CSM_CUDA(cudaEventCreate(&tune_ev_[i]));
+    }
     CSM_CUDA(dalloc(&d_ctrl_, 1));
     CSM_CUDA(dalloc(&d_misc_, 8));
     CSM_CUDA(cudaMallocHost(&h_counts_, sizeof(unsigned long long) * 64));
@@ -108,6 +149,8 @@ Engine::~Engine() {
     if (h_counts_) cudaFreeHost(h_counts_);
     if (h_ctrl_) cudaFreeHost(h_ctrl_);
     for (auto &e : ev_)
+        if (e) cudaEventDestroy(e);
+    for (auto &e : tune_ev_)
         if (e) cudaEventDestroy(e);
     if (stream_) cudaStreamDestroy(stream_);
 }
@@ -353,7 +396,7 @@ csm_status Engine::load_graph(uint32_t nv, const uint32_t *vlabel, uint64_t ne, 
     sc_.ticket_prefix = d_ticket_prefix_;
     const unsigned long long fbytes = cfg_.frontier_bytes ? cfg_.frontier_bytes : (1ull << 30);
     frontier_cap_ = std::max<unsigned long long>(1024, fbytes / 2 / sizeof(WorkItem));
-    if (opt_.search_strategy >= 2) {
+    if (opt_.search_strategy >= 2 || cfg_.autotune_batches > 0) {
         CSM_CUDA(dalloc(&d_frontier_[0], frontier_cap_));
         CSM_CUDA(dalloc(&d_frontier_[1], frontier_cap_));
     }
@@ -411,6 +454,30 @@ csm_status Engine::ensure_batch_capacity(uint64_t n) {
 
 csm_status Engine::apply_host(uint64_t n, const uint32_t *src, const uint32_t *dst, const uint32_t *elabel,
                               const uint8_t *is_delete, csm_batch_result *out) {
+    return apply_host_on(stream_, n, src, dst, elabel, is_delete, out);
+}
+
+csm_status Engine::apply_host_ctx(const ExecContext &ctx, uint64_t n, const uint32_t *src, const uint32_t *dst,
+                                  const uint32_t *elabel, const uint8_t *is_delete, csm_batch_result *out) {
+    if (ctx.frontier_cap && (!ctx.frontier[0] || !ctx.frontier[1]))
+        return fail(CSM_ERR_INVALID_ARG, "frontier buffers missing");
+    const EnumScratch saved = sc_;
+    WorkItem *f0 = d_frontier_[0], *f1 = d_frontier_[1];
+    const unsigned long long fcap = frontier_cap_;
+    sc_ = ctx.scratch;
+    d_frontier_[0] = ctx.frontier[0];
+    d_frontier_[1] = ctx.frontier[1];
+    frontier_cap_ = ctx.frontier_cap;
+    const csm_status st = apply_host_on(ctx.stream ? ctx.stream : stream_, n, src, dst, elabel, is_delete, out);
+    sc_ = saved;
+    d_frontier_[0] = f0;
+    d_frontier_[1] = f1;
+    frontier_cap_ = fcap;
+    return st;
+}
+
+csm_status Engine::apply_host_on(cudaStream_t s, uint64_t n, const uint32_t *src, const uint32_t *dst,
+                                 const uint32_t *elabel, const uint8_t *is_delete, csm_batch_result *out) {
     if (!graph_loaded_) return fail(CSM_ERR_STATE, "load the data graph first");
     if (poisoned_) return fail(CSM_ERR_STATE, "the engine failed an earlier batch; recreate it");
     if (n && (!src || !dst || !elabel)) return fail(CSM_ERR_INVALID_ARG, "null update array");
@@ -420,16 +487,15 @@ csm_status Engine::apply_host(uint64_t n, const uint32_t *src, const uint32_t *d
     if (is_delete)
         for (uint64_t i = 0; i < n && !has_delete; i++) has_delete = is_delete[i] != 0;
     // Timed from the first host->device copy (technique_permutation.h:123 includes the H2D).
-    CSM_CUDA(cudaEventRecord(ev_[0], stream_));
+    CSM_CUDA(cudaEventRecord(ev_[0], s));
     if (n) {
-        CSM_CUDA(cudaMemcpyAsync(d_upd_src_, src, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, stream_));
-        CSM_CUDA(cudaMemcpyAsync(d_upd_dst_, dst, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, stream_));
-        CSM_CUDA(cudaMemcpyAsync(d_upd_lab_, elabel, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, stream_));
+        CSM_CUDA(cudaMemcpyAsync(d_upd_src_, src, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, s));
+        CSM_CUDA(cudaMemcpyAsync(d_upd_dst_, dst, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, s));
+        CSM_CUDA(cudaMemcpyAsync(d_upd_lab_, elabel, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, s));
         if (has_delete)
-            CSM_CUDA(cudaMemcpyAsync(d_upd_del_, is_delete, n, cudaMemcpyHostToDevice, stream_));
+            CSM_CUDA(cudaMemcpyAsync(d_upd_del_, is_delete, n, cudaMemcpyHostToDevice, s));
     }
-    return run_batch(n, d_upd_src_, d_upd_dst_, d_upd_lab_, has_delete ? d_upd_del_ : nullptr, has_delete, stream_,
-                     out);
+    return run_batch(n, d_upd_src_, d_upd_dst_, d_upd_lab_, has_delete ? d_upd_del_ : nullptr, has_delete, s, out);
 }
 
 csm_status Engine::apply_device(uint64_t n, const uint32_t *src, const uint32_t *dst, const uint32_t *elabel,
@@ -471,6 +537,7 @@ csm_status Engine::run_batch(uint64_t n, const uint32_t *src, const uint32_t *ds
     const uint32_t np = (uint32_t)plans_.size();
     rows_valid_ = false;
     phase_ran_[0] = phase_ran_[1] = false;
+    last_frontier_rows_ = 0;
     CSM_CUDA(cudaMemsetAsync(bs_.nheads, 0, sizeof(unsigned int), s));
     CSM_CUDA(cudaMemsetAsync(bs_.counters, 0, 2 * sizeof(unsigned long long), s));
     CSM_CUDA(cudaMemsetAsync(bs_.error, 0, sizeof(unsigned int), s));
@@ -494,8 +561,25 @@ csm_status Engine::run_batch(uint64_t n, const uint32_t *src, const uint32_t *ds
         store_insert(m, d_keys_, kl_, g_, bs_, s);
         store_nlf_update(m, d_keys_, kl_, g_, bs_, nt, s);
         stats_.kernel_launches += 2;
-        csm_status st = enumerate_phase(CSM_PHASE_INS, m, s);
-        if (st != CSM_OK) return st;
+        csm_status st = CSM_OK;
+        if (tune_left_ > 0 && !no_alloc_ && cfg_.materialize_rows == 0) {
+            // Autotuning: the insertion phase runs once per candidate configuration (it does
+            // not change the graph, so every run counts the same matches); each run is timed.
+            const LaunchConfig keep = lc_;
+            for (size_t c = 0; c < tune_cands_.size(); c++) {
+                set_launch_config(tune_cands_[c]);
+                CSM_CUDA(cudaMemsetAsync(d_counts_ + np, 0, sizeof(unsigned long long) * np, s));
+                CSM_CUDA(cudaEventRecord(tune_ev_[2 * c], s));
+                st = enumerate_phase(CSM_PHASE_INS, m, s);
+                if (st != CSM_OK) return st;
+                CSM_CUDA(cudaEventRecord(tune_ev_[2 * c + 1], s));
+            }
+            set_launch_config(keep);
+            tuned_this_batch_ = true;
+        } else {
+            st = enumerate_phase(CSM_PHASE_INS, m, s);
+            if (st != CSM_OK) return st;
+        }
         store_clear_ins(m, d_keys_, kl_, g_, bs_, s);
         stats_.kernel_launches++;
     }
@@ -537,6 +621,20 @@ csm_status Engine::run_batch(uint64_t n, const uint32_t *src, const uint32_t *ds
     }
     float total_ms = 0.f, enum_ms = 0.f;
     CSM_CUDA(cudaEventElapsedTime(&total_ms, ev_[0], ev_[1]));
+    if (tuned_this_batch_) {
+        tuned_this_batch_ = false;
+        for (size_t c = 0; c < tune_cands_.size(); c++) {
+            float t = 0.f;
+            CSM_CUDA(cudaEventElapsedTime(&t, tune_ev_[2 * c], tune_ev_[2 * c + 1]));
+            tune_ms_[c] += t;
+        }
+        if (--tune_left_ == 0) {
+            size_t best = 0;
+            for (size_t c = 1; c < tune_cands_.size(); c++)
+                if (tune_ms_[c] < tune_ms_[best]) best = c;
+            set_launch_config(tune_cands_[best]);
+        }
+    }
     for (int ph = 0; ph < 2; ph++) {
         if (!phase_ran_[ph]) continue;
         float t = 0.f;
@@ -597,7 +695,7 @@ csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
     P.qcap = sc_.qcap;
     P.ctrl = sc_.ctrl;
     P.counts = d_counts_ + (phase == CSM_PHASE_INS ? np : 0);
-    P.steal_min = cfg_.steal_chunk > 0 ? (uint32_t)cfg_.steal_chunk : 64u;
+    P.steal_min = lc_.steal_chunk;
     // An idle warp leaves as soon as no warp holds work; the bound (about a minute of
     // polling) only ends the wait if that never happens.
     P.idle_limit = 1u << 24;
@@ -606,12 +704,12 @@ csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
     P.rows = d_rows_;
     P.row_cap = row_cap_;
     const bool rows = cfg_.materialize_rows > 0;
-    const int strategy = opt_.search_strategy;
+    const int strategy = lc_.strategy;
     const int ph = phase == CSM_PHASE_INS ? 1 : 0;
     phase_ran_[ph] = true;
     CSM_CUDA(cudaEventRecord(ev_[2 + 2 * ph], s));
 
-    launch_ctrl_reset(sc_.ctrl, total_warps, ++epoch_, 0, s);
+    launch_ctrl_reset(sc_.ctrl, total_warps, next_epoch(), 0, s);
     launch_seed_tickets(d_plans_, np, d_keys_, m, kl_, sc_.seed_lo, sc_.ticket_prefix, sc_.ctrl, s);
     stats_.kernel_launches += 3;
     const WorkItem *frontier = nullptr;
@@ -625,7 +723,7 @@ csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
                                  cudaMemcpyDeviceToHost, s));
         CSM_CUDA(cudaStreamSynchronize(s));
         unsigned long long cur = h_counts_[2 * np + 4] * 32;  // seed candidates (upper bound)
-        const unsigned long long target = 8ull * total_warps;
+        const unsigned long long target = (unsigned long long)lc_.frontier_mult * total_warps;
         int buf = 0;
         for (int level = 0; level < CSM_MAXQV; level++) {
             if (strategy == 2 && cur >= target) break;
@@ -647,7 +745,7 @@ csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
             X.frontier = frontier;
             X.expand_out = d_frontier_[buf];
             X.expand_cap = frontier_cap_;
-            if (frontier) launch_ctrl_reset(sc_.ctrl, total_warps, ++epoch_, nfront, s);
+            if (frontier) launch_ctrl_reset(sc_.ctrl, total_warps, next_epoch(), nfront, s);
             launch_enumerate(X, blocks_, warps_per_block_, occupancy_, s);
             stats_.enum_launches++;
             stats_.kernel_launches++;
@@ -659,6 +757,7 @@ csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
             const bool grew = rows_out != nfront || frontier == nullptr;
             frontier = d_frontier_[buf];
             nfront = rows_out;
+            last_frontier_rows_ = std::max(last_frontier_rows_, nfront);
             buf ^= 1;
             cur = nfront;
             if (!grew) break;
@@ -669,7 +768,7 @@ csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
     D.donate = (strategy == 0 || strategy == 2) ? 1u : 0u;
     if (frontier) {
         D.frontier = frontier;
-        launch_ctrl_reset(sc_.ctrl, total_warps, ++epoch_, nfront, s);
+        launch_ctrl_reset(sc_.ctrl, total_warps, next_epoch(), nfront, s);
         stats_.kernel_launches++;
     }
     launch_enumerate(D, blocks_, warps_per_block_, occupancy_, s);

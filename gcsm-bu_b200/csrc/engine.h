@@ -27,6 +27,28 @@ struct EnumScratch {
     uint32_t qcap = 0;
     uint32_t *seed_lo = nullptr;
     uint32_t *ticket_prefix = nullptr;
+    // Launch epoch counter of this scratch (the ready flags are valid for one epoch); null:
+    // the engine's own counter, which is right when the scratch serves this engine alone or
+    // its ready flags are cleared before the batch.
+    uint32_t *epoch = nullptr;
+};
+
+// Resources lent to the engine for one batch: enumeration scratch, two semi-BFS frontier
+// buffers of frontier_cap items (a cap of 0 means depth-first search only) and the stream.
+struct ExecContext {
+    EnumScratch scratch;
+    WorkItem *frontier[2] = {nullptr, nullptr};
+    unsigned long long frontier_cap = 0;
+    cudaStream_t stream = nullptr;
+};
+
+// One launch configuration of the enumeration (what the autotuner varies).
+struct LaunchConfig {
+    int strategy;          // search strategy 0..3
+    uint32_t steal_chunk;  // smallest candidate range split by donation
+    int warps_per_block;
+    int occupancy;         // kernel variant: resident 256-thread blocks per SM
+    uint32_t frontier_mult;  // semi-BFS stops once the frontier holds this many items per warp
 };
 
 struct Options {
@@ -60,7 +82,18 @@ class Engine {
     csm_status apply_device_noalloc(uint64_t n, const uint32_t *src, const uint32_t *dst, const uint32_t *elabel,
                                     const uint8_t *is_delete, cudaStream_t stream, const EnumScratch &scratch,
                                     csm_batch_result *out);
+    // The host-array batch pipeline on borrowed scratch, frontier and stream (the serving loop
+    // runs many engines on a few slots this way).
+    csm_status apply_host_ctx(const ExecContext &ctx, uint64_t n, const uint32_t *src, const uint32_t *dst,
+                              const uint32_t *elabel, const uint8_t *is_delete, csm_batch_result *out);
+    // Largest semi-BFS frontier (items) the last batch wrote.
+    unsigned long long last_frontier_rows() const { return last_frontier_rows_; }
     uint32_t num_plans() const { return (uint32_t)plans_.size(); }
+    bool graph_loaded() const { return graph_loaded_; }
+    // Warps of one enumeration launch (frontier estimates scale with it).
+    uint64_t enum_warps() const { return (uint64_t)blocks_ * (uint64_t)warps_per_block_; }
+    // Search strategy of the launch configuration in use (0..3).
+    int strategy() const { return lc_.strategy; }
     uint64_t batch_capacity() const { return batch_cap_; }
     int device() const { return device_; }
     cudaStream_t stream() const { return stream_; }
@@ -135,6 +168,10 @@ class Engine {
     uint32_t *d_ready_ = nullptr;
     uint32_t qcap_ = 0;
     uint32_t epoch_ = 0;
+    unsigned long long last_frontier_rows_ = 0;
+    uint32_t next_epoch() { return sc_.epoch ? ++*sc_.epoch : ++epoch_; }
+    csm_status apply_host_on(cudaStream_t s, uint64_t n, const uint32_t *src, const uint32_t *dst,
+                             const uint32_t *elabel, const uint8_t *is_delete, csm_batch_result *out);
     uint32_t *d_seed_lo_ = nullptr;       // 3 * nplans
     uint32_t *d_ticket_prefix_ = nullptr; // nplans + 1
     unsigned long long *d_counts_ = nullptr;  // per plan, per phase (2 * nplans)
@@ -151,6 +188,13 @@ class Engine {
     int warps_per_block_ = 8;
     int occupancy_ = 4;                       // enumeration kernel variant (blocks per SM)
     int blocks_ = 0;
+    LaunchConfig lc_{};                       // configuration in use
+    std::vector<LaunchConfig> tune_cands_;    // autotuner candidates
+    std::vector<double> tune_ms_;             // accumulated enumeration time per candidate
+    int tune_left_ = 0;                       // batches still to tune on
+    bool tuned_this_batch_ = false;
+    cudaEvent_t tune_ev_[32] = {};
+    void set_launch_config(const LaunchConfig &c);
 
     // Results of the last batch.
     std::vector<uint64_t> last_counts_;   // 2 * nplans

@@ -73,7 +73,9 @@ typedef struct csm_config {
     int32_t steal_chunk;            /* minimum candidate range split by work donation; 0 = auto */
     int32_t occupancy;              /* enumeration kernel built for 4, 5 or 6 resident 256-thread
                                        blocks per SM (fewer registers per thread); 0 = 4 */
-    int32_t reserved[4];
+    int32_t autotune_batches;       /* >0: over the first batches, time the enumeration under every
+                                       candidate launch configuration and keep the fastest */
+    int32_t reserved[3];
 } csm_config;
 
 /* Per-query result of one batch. */
@@ -102,7 +104,10 @@ typedef struct csm_stats {
     uint64_t pool_used;             /* adjacency pool entries in use */
     uint64_t pool_capacity;
     uint64_t compactions;           /* pool compactions (slack re-layout) */
-    uint64_t reserved[4];
+    uint64_t tuned_strategy;        /* launch configuration in use (chosen by the autotuner, or */
+    uint64_t tuned_steal_chunk;     /* the configured one) */
+    uint64_t tuned_warps_per_block;
+    uint64_t tuned_occupancy;
 } csm_stats;
 
 /* Fills `cfg` with the defaults (algorithm 0 with all switches on, as main.cpp). */

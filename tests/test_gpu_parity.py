@@ -145,3 +145,21 @@ def test_launch_shapes_and_steal_chunk():
     w = small_workload("c2", scale=0.003, batch=3000, nqueries=4)
     for bps, wpb, sc in ((1, 1, 32), (2, 4, 128), (8, 8, 64)):
         check_stream(w, blocks_per_sm=bps, warps_per_block=wpb, steal_chunk=sc, search_strategy=0)
+
+
+def test_autotune_keeps_counts_and_reports_choice():
+    # Tuning re-runs the insertion phase under each candidate configuration; the counts of
+    # the tuned batches and of the batches after them must not change.
+    w = small_workload("c2", scale=0.003, batch=3000, nqueries=3)
+    check_stream(w, search_strategy=2, autotune_batches=2)
+    eng = csm.Engine(search_strategy=2, autotune_batches=2)
+    eng.load_query(w.queries[0])
+    eng.load_graph(w.data)
+    for b in w.batches[:3]:
+        eng.apply(b)
+    st = eng.stats()
+    assert st.tuned_strategy in (0, 2)
+    assert st.tuned_steal_chunk in (64, 256)
+    assert st.tuned_warps_per_block in (4, 8)
+    assert st.tuned_occupancy in (4, 5)
+    eng.close()
