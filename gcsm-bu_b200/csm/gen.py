@@ -209,10 +209,21 @@ class Workload:
     meta: dict = field(default_factory=dict)
 
 
+def loguniform_cuts(total: int, lo: int, hi: int, seed: int) -> List[int]:
+    """Batch boundaries for `total` updates with sizes drawn log-uniformly from [lo, hi]."""
+    rng = np.random.default_rng(seed)
+    cuts, at = [0], 0
+    while at < total:
+        at = min(total, at + int(round(np.exp(rng.uniform(np.log(lo), np.log(hi))))))
+        cuts.append(at)
+    return cuts
+
+
 def make_stream(n: int, s: np.ndarray, d: np.ndarray, el: np.ndarray, rng: np.random.Generator, n_ins: int,
-                n_del: int, batch: int, holdout: float = 0.1):
+                n_del: int, batch: int, holdout: float = 0.1, cuts: Optional[List[int]] = None):
     """Splits the edges into an initial graph and a held-out pool; the stream inserts n_ins pool
-    edges and deletes n_del initial edges, randomly interleaved, cut into batches."""
+    edges and deletes n_del initial edges, randomly interleaved, cut into batches of `batch`
+    updates (or at the given boundaries)."""
     m = len(s)
     perm = rng.permutation(m)
     nh = int(round(m * holdout))
@@ -230,8 +241,10 @@ def make_stream(n: int, s: np.ndarray, d: np.ndarray, el: np.ndarray, rng: np.ra
     us = np.where(flip, d[ops], s[ops]).astype(np.uint32)
     vs = np.where(flip, s[ops], d[ops]).astype(np.uint32)
     batches = []
-    for b0 in range(0, len(ops), batch):
-        sl = slice(b0, b0 + batch)
+    if cuts is None:
+        cuts = list(range(0, len(ops), batch)) + [len(ops)]
+    for b0, b1 in zip(cuts[:-1], cuts[1:]):
+        sl = slice(b0, b1)
         batches.append(Batch(us[sl], vs[sl], el[ops[sl]].astype(np.uint32), isdel[sl] if n_del else None))
     data = DataGraph(None, s[init], d[init], el[init])
     return data, batches
@@ -251,8 +264,9 @@ CONFIGS = {
     "c4": dict(n=400_000, m=2_400_000, gamma=2.1, nvl=6, vzipf=1.0, nel=1, ezipf=None, cap=True, n_ins=216_000,
                n_del=24_000, batch=65_536, queries="mixed64"),
     # Serving: Netflow-shaped multi-label graph, 32 queries of 4..10 vertices.
+    # Batch sizes are log-uniform in [1k, 256k] (batch_range); `batch` is the largest.
     "c5": dict(n=3_000_000, m=20_000_000, gamma=2.1, nvl=8, vzipf=None, nel=16, ezipf=1.1, cap=True,
-               n_ins=700_000, n_del=300_000, batch=65_536, queries="mixed32"),
+               n_ins=700_000, n_del=300_000, batch=262_144, batch_range=(1_024, 262_144), queries="mixed32"),
 }
 
 
@@ -272,7 +286,12 @@ def make_workload(name: str, cfg: Optional[dict] = None, seed: Optional[int] = N
     s, d = chung_lu(cfg["n"], cfg["m"], cfg["gamma"], rng, cap=cfg["cap"])
     vlab = draw_labels(cfg["n"], cfg["nvl"], rng, cfg["vzipf"])
     el = draw_labels(len(s), cfg["nel"], rng, cfg["ezipf"]) if cfg["nel"] > 1 else np.zeros(len(s), dtype=np.uint32)
-    data, batches = make_stream(cfg["n"], s, d, el, rng, cfg["n_ins"], cfg["n_del"], cfg["batch"])
+    cuts = None
+    if cfg.get("batch_range"):
+        lo, hi = cfg["batch_range"]
+        hi = min(hi, cfg["batch"])
+        cuts = loguniform_cuts(cfg["n_ins"] + cfg["n_del"], min(lo, hi), hi, seed + 7919)
+    data, batches = make_stream(cfg["n"], s, d, el, rng, cfg["n_ins"], cfg["n_del"], cfg["batch"], cuts=cuts)
     data.vlabels = vlab
     adj = Adjacency(cfg["n"], data.src, data.dst, data.elabels)
     qspec = cfg["queries"]

@@ -17,13 +17,17 @@ def ensure_built():
         subprocess.run(["make", "-s", "-j8", "-C", os.path.join(ROOT, "gcsm-bu_b200")], check=True)
 
 
-def declared_symbols():
-    text = open(os.path.join(ROOT, "include", "csm.h")).read()
-    return sorted(set(re.findall(r"\b(csm_[a-z_]+)\s*\(", text)))
+def declared_symbols(headers=("csm.h", "csm_server.h")):
+    found = set()
+    for h in headers:
+        text = open(os.path.join(ROOT, "include", h)).read()
+        found |= set(re.findall(r"\b(csm_[a-z_]+)\s*\(", text))
+    return sorted(found)
 
 
 def test_header_matches_python_binding():
-    assert declared_symbols() == sorted(csm.EXPORTED)
+    assert declared_symbols(("csm.h",)) == sorted(csm.EXPORTED)
+    assert declared_symbols(("csm_server.h",)) == sorted(csm.SERVER_EXPORTED)
 
 
 def test_library_exports_every_declared_symbol():
@@ -58,3 +62,16 @@ def test_struct_layouts():
     assert ctypes.sizeof(csm.CsmConfig) == 4 * 8 + 8 * 4 + 4 * 8
     assert ctypes.sizeof(csm.CsmBatchResult) == 64
     assert ctypes.sizeof(csm.CsmStats) == 16 * 8
+    assert ctypes.sizeof(csm.CsmServerConfig) == 4 + 4 + 8 + 8 + 4 + 7 * 4
+    assert ctypes.sizeof(csm.CsmRequestInfo) == 8 + 7 * 8
+    assert ctypes.sizeof(csm.CsmServerStats) == 12 * 8
+
+
+def test_server_create_fails_loudly_without_gpu():
+    ensure_built()
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(csm.CsmError) as ei:
+        csm.Server()
+    assert ei.value.code == -8
