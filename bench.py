@@ -61,6 +61,14 @@ def parse():
     return ap.parse_args()
 
 
+_T0 = time.perf_counter()
+
+
+def log(msg):
+    """Progress on stderr (the JSON line alone goes to stdout)."""
+    print(f"[bench {time.perf_counter() - _T0:8.1f}s] {msg}", file=sys.stderr, flush=True)
+
+
 def inverse(b):
     from csm import Batch
     dl = b.is_delete if b.is_delete is not None else np.zeros(len(b.src), dtype=np.uint8)
@@ -276,9 +284,11 @@ def run_ours(args, w, world, rank, local):
     warm, timed, timed_e2e = plan[: args.warmup], plan[args.warmup: args.warmup + args.steps], plan[args.warmup + args.steps:]
     for _, b in plan:
         on_device(b)
+    log("engines loaded")
     for qi, b in warm:
         apply_dev(qi, b)
     torch.cuda.synchronize(dev)
+    log("warm-up done")
     for e in engines:
         e.reset_stats()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -414,6 +424,7 @@ def run_batched(args, w, world, rank, local):
     for q in w.queries:
         eng.load_query(q)
     eng.load_graph(w.data)
+    log("batched engine loaded")
     seq = step_batches(w, args.warmup + 2 * args.steps)
     warm, timed, timed_e2e = seq[: args.warmup], seq[args.warmup: args.warmup + args.steps], seq[args.warmup + args.steps:]
     dev_cache = {}
@@ -426,7 +437,8 @@ def run_batched(args, w, world, rank, local):
         return e.apply_device(len(b.src), s.data_ptr(), d.data_ptr(), l.data_ptr(), dl.data_ptr(), stream.cuda_stream)
 
     for b in warm:
-        apply_dev(eng, b)
+        res = apply_dev(eng, b)
+        log(f"warm-up batch: {res[0].latency_ns / 1e6:.1f} ms, {sum(r.positive + r.negative for r in res)} matches")
     torch.cuda.synchronize(dev)
     eng.reset_stats()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -441,6 +453,7 @@ def run_batched(args, w, world, rank, local):
             matches += sum(r.positive + r.negative for r in res)
             upd += len(b.src)
             lat.append(res[0].latency_ns / 1e6)
+            log(f"timed batch: {lat[-1]:.1f} ms")
         ev1.record(stream)
         torch.cuda.synchronize(dev)
     barrier(world)
@@ -486,6 +499,7 @@ def run_batched(args, w, world, rank, local):
         plain_matches += sum(p + n for p, n in got)
         identical &= all(got[i] == per_batch[i][qi] for i in range(nplain))
         e.close()
+        log(f"plain query {qi}: total {plain_t:.2f} s so far")
     plain_tmax = max_over_ranks(plain_t, world, dev)
     if rank != 0:
         return
@@ -590,7 +604,9 @@ def run_served(args, w, world, rank, local):
             infos.append(info)
         return rows, infos
 
+    log(f"server: {len(groups)} tenants loaded")
     collect([srv.submit(b) for b in warm])
+    log("served warm-up done")
     rng = np.random.default_rng(4242)
     gaps = rng.exponential(1.0 / args.rate, size=len(poisson))
     barrier(world)
@@ -604,9 +620,11 @@ def run_served(args, w, world, rank, local):
             ids.append(srv.submit(b))
         rows_p, infos_p = collect(ids)
         span_p = (max(i.done_ns for i in infos_p) - min(i.arrival_ns for i in infos_p)) / 1e9
+        log(f"poisson phase: {span_p:.2f} s")
         ids = [srv.submit(b) for b in burst]
         rows_b, infos_b = collect(ids)
         span_b = (max(i.done_ns for i in infos_b) - min(i.arrival_ns for i in infos_b)) / 1e9
+        log(f"burst phase: {span_b:.2f} s")
     barrier(world)
     span_b_max = max_over_ranks(span_b, world, dev)
     lat = [(i.done_ns - i.arrival_ns) / 1e6 for i in infos_p]
@@ -647,6 +665,7 @@ def run_served(args, w, world, rank, local):
         plain_matches += sum(p + n for p, n in got)
         identical &= all(got[i] == rows_b[i][qi] for i in range(nplain))
         e.close()
+        log(f"plain query {qi}: total {plain_t:.2f} s so far")
     plain_tmax = max_over_ranks(plain_t, world, dev)
     if rank != 0:
         return
@@ -705,7 +724,9 @@ def main():
     cfg = gen.scaled(args.config, args.scale) if args.scale != 1.0 else dict(gen.CONFIGS[args.config])
     if args.batch:
         cfg["batch"] = args.batch
+    log(f"generating {args.config} (scale {args.scale})")
     w = gen.make_workload(args.config, cfg, nqueries=args.nqueries)
+    log(f"workload: {len(w.data.src)} edges, {len(w.batches)} batches, {len(w.queries)} queries")
     if args.impl == "reference":
         run_reference(args, w, world, rank)
     elif args.form == "batched":

@@ -67,7 +67,8 @@ class CsmConfig(ctypes.Structure):
         ("steal_chunk", ctypes.c_int32),
         ("occupancy", ctypes.c_int32),
         ("autotune_batches", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 3),
+        ("cuda_graphs", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 2),
     ]
 
 
@@ -88,7 +89,8 @@ class CsmStats(ctypes.Structure):
     _fields_ = [(name, ctypes.c_uint64) for name in (
         "batches", "enum_launches", "kernel_launches", "enum_scan_entries", "enum_probes",
         "enum_tail_lists", "donations", "enum_ns", "apply_ns", "pool_used", "pool_capacity",
-        "compactions", "tuned_strategy", "tuned_steal_chunk", "tuned_warps_per_block", "tuned_occupancy")]
+        "compactions", "tuned_strategy", "tuned_steal_chunk", "tuned_warps_per_block", "tuned_occupancy",
+        "graph_launches")] + [("reserved", ctypes.c_uint64 * 3)]
 
 
 class CsmError(RuntimeError):

@@ -130,6 +130,7 @@ csm_status Engine::init() {
         for (size_t i = 0; i < 2 * tune_cands_.size(); i++) CSM_CUDA(cudaEventCreate(&tune_ev_[i]));
     }
     CSM_CUDA(dalloc(&d_ctrl_, 1));
+    CSM_CUDA(cudaMemset(d_ctrl_, 0, sizeof(EnumControl)));
     CSM_CUDA(dalloc(&d_misc_, 8));
     CSM_CUDA(cudaMallocHost(&h_counts_, sizeof(unsigned long long) * 64));
     CSM_CUDA(cudaMallocHost(&h_ctrl_, sizeof(EnumControl) * 2));
@@ -138,6 +139,7 @@ csm_status Engine::init() {
 
 Engine::~Engine() {
     if (stream_) cudaStreamSynchronize(stream_);
+    clear_graphs();
     void *dev[] = {d_elab_raw_, d_rel_table_, d_spec_begin_, d_specs_, d_bits_, g_.meta, g_.cap, g_.pool, g_.pool_top,
                    g_.vlab, d_plans_, d_terms_, d_upd_src_, d_upd_dst_, d_upd_lab_, d_upd_del_, d_keys_raw_, d_keys_,
                    d_sort_temp_, bs_.eff, bs_.heads, bs_.nheads, bs_.seg_nins, bs_.seg_ndel, bs_.seg_end, bs_.scr_y,
@@ -418,6 +420,8 @@ csm_status Engine::load_graph(uint32_t nv, const uint32_t *vlabel, uint64_t ne, 
 
 csm_status Engine::ensure_batch_capacity(uint64_t n) {
     if (n <= batch_cap_) return CSM_OK;
+    clear_graphs();
+    graph_gen_++;
     uint64_t cap = std::max<uint64_t>(n, batch_cap_ * 2);
     if (2 * cap >= 0x7FFFFFFFull) return fail(CSM_ERR_LIMIT, "batch too large (limit 2^30 updates)");
     CSM_CUDA(cudaStreamSynchronize(stream_));
@@ -507,6 +511,15 @@ csm_status Engine::apply_device(uint64_t n, const uint32_t *src, const uint32_t 
     if (st != CSM_OK) return st;
     cudaStream_t s = stream ? stream : stream_;
     CSM_CUDA(cudaEventRecord(ev_[0], s));
+    if (graphs_on() && n) {
+        // The replayed graph reads the engine's own update buffers.
+        CSM_CUDA(cudaMemcpyAsync(d_upd_src_, src, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, s));
+        CSM_CUDA(cudaMemcpyAsync(d_upd_dst_, dst, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, s));
+        CSM_CUDA(cudaMemcpyAsync(d_upd_lab_, elabel, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, s));
+        if (is_delete) CSM_CUDA(cudaMemcpyAsync(d_upd_del_, is_delete, n, cudaMemcpyDeviceToDevice, s));
+        return run_batch(n, d_upd_src_, d_upd_dst_, d_upd_lab_, is_delete ? d_upd_del_ : nullptr, is_delete != nullptr,
+                         s, out);
+    }
     return run_batch(n, src, dst, elabel, is_delete, is_delete != nullptr, s, out);
 }
 
@@ -531,13 +544,10 @@ csm_status Engine::apply_device_noalloc(uint64_t n, const uint32_t *src, const u
     return st;
 }
 
-csm_status Engine::run_batch(uint64_t n, const uint32_t *src, const uint32_t *dst, const uint32_t *elabel,
-                             const uint8_t *is_delete, bool has_delete, cudaStream_t s, csm_batch_result *out) {
+csm_status Engine::enqueue_batch(uint64_t n, const uint32_t *src, const uint32_t *dst, const uint32_t *elabel,
+                                 const uint8_t *is_delete, bool has_delete, bool tuning, cudaStream_t s) {
     const uint32_t m = (uint32_t)(2 * n);
     const uint32_t np = (uint32_t)plans_.size();
-    rows_valid_ = false;
-    phase_ran_[0] = phase_ran_[1] = false;
-    last_frontier_rows_ = 0;
     CSM_CUDA(cudaMemsetAsync(bs_.nheads, 0, sizeof(unsigned int), s));
     CSM_CUDA(cudaMemsetAsync(bs_.counters, 0, 2 * sizeof(unsigned long long), s));
     CSM_CUDA(cudaMemsetAsync(bs_.error, 0, sizeof(unsigned int), s));
@@ -562,7 +572,7 @@ csm_status Engine::run_batch(uint64_t n, const uint32_t *src, const uint32_t *ds
         store_nlf_update(m, d_keys_, kl_, g_, bs_, nt, s);
         stats_.kernel_launches += 2;
         csm_status st = CSM_OK;
-        if (tune_left_ > 0 && !no_alloc_ && cfg_.materialize_rows == 0) {
+        if (tuning) {
             // Autotuning: the insertion phase runs once per candidate configuration (it does
             // not change the graph, so every run counts the same matches); each run is timed.
             const LaunchConfig keep = lc_;
@@ -583,15 +593,92 @@ csm_status Engine::run_batch(uint64_t n, const uint32_t *src, const uint32_t *ds
         store_clear_ins(m, d_keys_, kl_, g_, bs_, s);
         stats_.kernel_launches++;
     }
+    return enqueue_readback(s);
+}
+
+// The end of a batch's device work: the timing event and the copies the host reads after the
+// batch's single synchronisation (counts, edge counters, pool top, error bits).
+csm_status Engine::enqueue_readback(cudaStream_t s) {
+    const uint32_t np = (uint32_t)plans_.size();
+    unsigned int *h_err = reinterpret_cast<unsigned int *>(h_counts_ + 2 * np + 3);
+    CSM_CUDA(cudaEventRecord(ev_[1], s));
+    CSM_CUDA(cudaMemcpyAsync(h_counts_, d_counts_, 2 * sizeof(unsigned long long) * np, cudaMemcpyDeviceToHost, s));
+    CSM_CUDA(cudaMemcpyAsync(h_counts_ + 2 * np, bs_.counters, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                             s));
+    CSM_CUDA(cudaMemcpyAsync(h_counts_ + 2 * np + 2, g_.pool_top, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                             s));
+    CSM_CUDA(cudaMemcpyAsync(h_err, bs_.error, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+    return CSM_OK;
+}
+
+// Replays the batch's device work from a CUDA graph captured for this batch size and launch
+// configuration (captured on first use; any reallocation of engine buffers starts a new one).
+csm_status Engine::launch_graph(uint64_t n, bool has_delete, cudaStream_t s) {
+    GraphKey key{n, has_delete, graph_gen_, lc_.strategy, lc_.steal_chunk, lc_.warps_per_block, lc_.occupancy, blocks_};
+    GraphEntry *hit = nullptr;
+    for (auto &g : graphs_)
+        if (g.key == key) hit = &g;
+    if (!hit) {
+        if (graphs_.size() >= 8) clear_graphs();
+        const Stats0 before{stats_.kernel_launches, stats_.enum_launches};
+        CSM_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+        const csm_status st = enqueue_batch(n, d_upd_src_, d_upd_dst_, d_upd_lab_, has_delete ? d_upd_del_ : nullptr,
+                                            has_delete, false, s);
+        cudaGraph_t g = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(s, &g);
+        if (st != CSM_OK) {
+            if (g) cudaGraphDestroy(g);
+            return st;
+        }
+        if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
+        GraphEntry e;
+        e.key = key;
+        const cudaError_t ie = cudaGraphInstantiate(&e.exec, g, 0);
+        cudaGraphDestroy(g);
+        if (ie != cudaSuccess) return cuda_fail(ie, "cudaGraphInstantiate");
+        e.kernels = stats_.kernel_launches - before.kernels;
+        e.enum_launches = stats_.enum_launches - before.enum_launches;
+        stats_.kernel_launches = before.kernels;
+        stats_.enum_launches = before.enum_launches;
+        graphs_.push_back(e);
+        hit = &graphs_.back();
+    }
+    CSM_CUDA(cudaGraphLaunch(hit->exec, s));
+    stats_.kernel_launches += hit->kernels;
+    stats_.enum_launches += hit->enum_launches;
+    stats_.graph_launches++;
+    if (n) phase_ran_[1] = true;
+    if (n && has_delete) phase_ran_[0] = true;
+    return CSM_OK;
+}
+
+void Engine::clear_graphs() {
+    for (auto &g : graphs_)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    graphs_.clear();
+}
+
+csm_status Engine::run_batch(uint64_t n, const uint32_t *src, const uint32_t *dst, const uint32_t *elabel,
+                             const uint8_t *is_delete, bool has_delete, cudaStream_t s, csm_batch_result *out) {
+    const uint32_t m = (uint32_t)(2 * n);
+    const uint32_t np = (uint32_t)plans_.size();
+    rows_valid_ = false;
+    phase_ran_[0] = phase_ran_[1] = false;
+    last_frontier_rows_ = 0;
+    NlfTables nt{d_spec_begin_, d_specs_, d_bits_, words_};
+    const bool tuning = tune_left_ > 0 && !no_alloc_ && cfg_.materialize_rows == 0;
+    csm_status est;
+    if (graphs_on() && !tuning && src == d_upd_src_)
+        est = launch_graph(n, has_delete, s);
+    else
+        est = enqueue_batch(n, src, dst, elabel, is_delete, has_delete, tuning, s);
+    if (est != CSM_OK) return est;
     unsigned int *h_err = reinterpret_cast<unsigned int *>(h_counts_ + 2 * np + 3);
     for (int attempt = 0;; attempt++) {
-        CSM_CUDA(cudaEventRecord(ev_[1], s));
-        CSM_CUDA(cudaMemcpyAsync(h_counts_, d_counts_, 2 * sizeof(unsigned long long) * np, cudaMemcpyDeviceToHost, s));
-        CSM_CUDA(cudaMemcpyAsync(h_counts_ + 2 * np, bs_.counters, 2 * sizeof(unsigned long long),
-                                 cudaMemcpyDeviceToHost, s));
-        CSM_CUDA(cudaMemcpyAsync(h_counts_ + 2 * np + 2, g_.pool_top, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
-                                 s));
-        CSM_CUDA(cudaMemcpyAsync(h_err, bs_.error, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+        if (attempt > 0) {
+            const csm_status rb = enqueue_readback(s);
+            if (rb != CSM_OK) return rb;
+        }
         CSM_CUDA(cudaStreamSynchronize(s));
         CSM_CUDA(cudaGetLastError());
         stats_.pool_used = h_counts_[2 * np + 2];
@@ -709,7 +796,7 @@ csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
     phase_ran_[ph] = true;
     CSM_CUDA(cudaEventRecord(ev_[2 + 2 * ph], s));
 
-    launch_ctrl_reset(sc_.ctrl, total_warps, next_epoch(), 0, s);
+    launch_ctrl_reset(sc_.ctrl, total_warps, 0, s);
     launch_seed_tickets(d_plans_, np, d_keys_, m, kl_, sc_.seed_lo, sc_.ticket_prefix, sc_.ctrl, s);
     stats_.kernel_launches += 3;
     const WorkItem *frontier = nullptr;
@@ -745,7 +832,7 @@ csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
             X.frontier = frontier;
             X.expand_out = d_frontier_[buf];
             X.expand_cap = frontier_cap_;
-            if (frontier) launch_ctrl_reset(sc_.ctrl, total_warps, next_epoch(), nfront, s);
+            if (frontier) launch_ctrl_reset(sc_.ctrl, total_warps, nfront, s);
             launch_enumerate(X, blocks_, warps_per_block_, occupancy_, s);
             stats_.enum_launches++;
             stats_.kernel_launches++;
@@ -768,7 +855,7 @@ csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
     D.donate = (strategy == 0 || strategy == 2) ? 1u : 0u;
     if (frontier) {
         D.frontier = frontier;
-        launch_ctrl_reset(sc_.ctrl, total_warps, next_epoch(), nfront, s);
+        launch_ctrl_reset(sc_.ctrl, total_warps, nfront, s);
         stats_.kernel_launches++;
     }
     launch_enumerate(D, blocks_, warps_per_block_, occupancy_, s);
@@ -813,6 +900,8 @@ csm_status Engine::maybe_compact(cudaStream_t s) {
             cudaFree(g_.pool);
             g_.pool = np;
             g_.pool_cap = new_cap;
+            clear_graphs();
+            graph_gen_++;
             stats_.pool_used = live;
             stats_.pool_capacity = new_cap;
             stats_.compactions++;

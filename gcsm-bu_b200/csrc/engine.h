@@ -27,10 +27,6 @@ struct EnumScratch {
     uint32_t qcap = 0;
     uint32_t *seed_lo = nullptr;
     uint32_t *ticket_prefix = nullptr;
-    // Launch epoch counter of this scratch (the ready flags are valid for one epoch); null:
-    // the engine's own counter, which is right when the scratch serves this engine alone or
-    // its ready flags are cleared before the batch.
-    uint32_t *epoch = nullptr;
 };
 
 // Resources lent to the engine for one batch: enumeration scratch, two semi-BFS frontier
@@ -167,9 +163,38 @@ class Engine {
     WorkItem *d_queue_ = nullptr;
     uint32_t *d_ready_ = nullptr;
     uint32_t qcap_ = 0;
-    uint32_t epoch_ = 0;
     unsigned long long last_frontier_rows_ = 0;
-    uint32_t next_epoch() { return sc_.epoch ? ++*sc_.epoch : ++epoch_; }
+    // CUDA graphs of whole batches (depth-first strategies), keyed by what the capture bakes in.
+    struct GraphKey {
+        uint64_t n;
+        bool del;
+        uint64_t gen;
+        int strategy;
+        uint32_t steal;
+        int wpb, occ, blocks;
+        bool operator==(const GraphKey &o) const {
+            return n == o.n && del == o.del && gen == o.gen && strategy == o.strategy && steal == o.steal &&
+                   wpb == o.wpb && occ == o.occ && blocks == o.blocks;
+        }
+    };
+    struct GraphEntry {
+        GraphKey key{};
+        cudaGraphExec_t exec = nullptr;
+        uint64_t kernels = 0, enum_launches = 0;
+    };
+    struct Stats0 {
+        uint64_t kernels, enum_launches;
+    };
+    std::vector<GraphEntry> graphs_;
+    uint64_t graph_gen_ = 0;  // bumped whenever a buffer a graph refers to is reallocated
+    bool graphs_on() const {
+        return cfg_.cuda_graphs && !no_alloc_ && lc_.strategy < 2 && cfg_.materialize_rows == 0;
+    }
+    csm_status enqueue_batch(uint64_t n, const uint32_t *src, const uint32_t *dst, const uint32_t *elabel,
+                             const uint8_t *is_delete, bool has_delete, bool tuning, cudaStream_t s);
+    csm_status enqueue_readback(cudaStream_t s);
+    csm_status launch_graph(uint64_t n, bool has_delete, cudaStream_t s);
+    void clear_graphs();
     csm_status apply_host_on(cudaStream_t s, uint64_t n, const uint32_t *src, const uint32_t *dst,
                              const uint32_t *elabel, const uint8_t *is_delete, csm_batch_result *out);
     uint32_t *d_seed_lo_ = nullptr;       // 3 * nplans

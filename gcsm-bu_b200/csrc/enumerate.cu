@@ -747,31 +747,48 @@ __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, unsign
             const uint32_t vmask = __ballot_sync(0xffffffffu, idx < S.hi[d]);
             const uint32_t target = __shfl_sync(0xffffffffu, cand, 31 - __clz(vmask));
             const uint32_t key_hi = (target + 1) << 1;
-            for (uint32_t k = 0; k < nbn; k++) {
-                if (k == piv) continue;
+            // The windows of up to four lists are read together (independent loads in flight
+            // at once), then each list is resolved in turn.
+            for (uint32_t k0 = 0; k0 < nbn; k0 += 4) {
                 if (!__any_sync(0xffffffffu, ok)) break;
-                const uint32_t slot = S.bnb[d] + k;
-                const uint32_t *L = P.g.pool + S.poff[slot];
-                const uint32_t c0 = S.cur[slot];
-                const uint32_t size = S.psz[slot];
-                uint32_t win = c0 + lane < size ? __ldg(L + c0 + lane) : 0xFFFFFFFFu;
-                const uint32_t below = __ballot_sync(0xffffffffu, win < key_hi);
-                uint32_t e = 0xFFFFFFFFu, hi;
-                if (below != 0xffffffffu) {
-                    // The window [c0, hi) fits in the 32 entries just read.
-                    hi = c0 + __popc(below);
-                    const uint32_t pos = shfl_lower_bound(win, cand << 1);
-                    const uint32_t got = __shfl_sync(0xffffffffu, win, pos);
-                    if ((got >> 1) == cand && got != 0xFFFFFFFFu) e = got;
-                } else {
-                    hi = warp_lower_bound(L, c0 + 32, size, key_hi, lane);
-                    if (ok) e = find_entry(L + c0, hi - c0, cand);
+                uint32_t win[4];
+#pragma unroll
+                for (uint32_t j = 0; j < 4; j++) {
+                    const uint32_t k = k0 + j;
+                    win[j] = 0xFFFFFFFFu;
+                    if (k < nbn && k != piv) {
+                        const uint32_t slot = S.bnb[d] + k;
+                        const uint32_t c0 = S.cur[slot];
+                        if (c0 + lane < S.psz[slot]) win[j] = __ldg(P.g.pool + S.poff[slot] + c0 + lane);
+                    }
                 }
-                if (ok) {
-                    probes++;
-                    ok = e != 0xFFFFFFFFu && !(((oldm >> k) & 1u) && (e & 1u));
+#pragma unroll
+                for (uint32_t j = 0; j < 4; j++) {
+                    const uint32_t k = k0 + j;
+                    if (k >= nbn || k == piv) continue;
+                    if (!__any_sync(0xffffffffu, ok)) break;
+                    const uint32_t slot = S.bnb[d] + k;
+                    const uint32_t *L = P.g.pool + S.poff[slot];
+                    const uint32_t c0 = S.cur[slot];
+                    const uint32_t size = S.psz[slot];
+                    const uint32_t below = __ballot_sync(0xffffffffu, win[j] < key_hi);
+                    uint32_t e = 0xFFFFFFFFu, hi;
+                    if (below != 0xffffffffu) {
+                        // The window [c0, hi) fits in the 32 entries just read.
+                        hi = c0 + __popc(below);
+                        const uint32_t pos = shfl_lower_bound(win[j], cand << 1);
+                        const uint32_t got = __shfl_sync(0xffffffffu, win[j], pos);
+                        if ((got >> 1) == cand && got != 0xFFFFFFFFu) e = got;
+                    } else {
+                        hi = warp_lower_bound(L, c0 + 32, size, key_hi, lane);
+                        if (ok) e = find_entry(L + c0, hi - c0, cand);
+                    }
+                    if (ok) {
+                        probes++;
+                        ok = e != 0xFFFFFFFFu && !(((oldm >> k) & 1u) && (e & 1u));
+                    }
+                    if (lane == 0) S.cur[slot] = hi;
                 }
-                if (lane == 0) S.cur[slot] = hi;
             }
             if (ok) ok = (nlf_word >> (cand & 31)) & 1u;
         }
@@ -971,7 +988,12 @@ __global__ void k_ticket_prefix(const uint32_t *chunks, uint32_t nplans, uint32_
     }
 }
 
-__global__ void k_ctrl_reset(EnumControl *ctrl, uint32_t active, uint32_t epoch, unsigned long long nticket) {
+// Resets the control block for one launch.  The launch epoch (which marks queue slots ready)
+// is the previous one plus one, kept on the device so that every launch on this scratch gets a
+// fresh epoch whichever engine, stream or replayed graph issues it.
+__global__ void k_ctrl_reset(EnumControl *ctrl, uint32_t active, unsigned long long nticket) {
+    uint32_t epoch = ctrl->epoch + 1u;
+    if (epoch == 0) epoch = 1;
     EnumControl c;
     memset(&c, 0, sizeof(c));
     c.active = active;
@@ -1047,9 +1069,8 @@ void launch_seed_tickets(const DevPlan *plans, uint32_t nplans, const unsigned l
     k_ticket_prefix<<<1, 1024, 0, s>>>(chunks, nplans, ticket_prefix, ctrl);
 }
 
-void launch_ctrl_reset(EnumControl *ctrl, uint32_t active, uint32_t epoch, unsigned long long nticket,
-                       cudaStream_t s) {
-    k_ctrl_reset<<<1, 1, 0, s>>>(ctrl, active, epoch, nticket);
+void launch_ctrl_reset(EnumControl *ctrl, uint32_t active, unsigned long long nticket, cudaStream_t s) {
+    k_ctrl_reset<<<1, 1, 0, s>>>(ctrl, active, nticket);
 }
 
 void launch_expand_bound(const EnumParams &p, const WorkItem *items, const unsigned long long *nitems,

@@ -122,8 +122,7 @@ void launch_enumerate(const EnumParams &p, int blocks, int warps_per_block, int 
 void launch_seed_tickets(const DevPlan *plans, uint32_t nplans, const unsigned long long *keys, uint32_t m,
                          KeyLayout kl, uint32_t *seed_lo, uint32_t *ticket_prefix, EnumControl *ctrl,
                          cudaStream_t s);
-void launch_ctrl_reset(EnumControl *ctrl, uint32_t active, uint32_t epoch, unsigned long long nticket,
-                       cudaStream_t s);
+void launch_ctrl_reset(EnumControl *ctrl, uint32_t active, unsigned long long nticket, cudaStream_t s);
 void launch_expand_bound(const EnumParams &p, const WorkItem *items, const unsigned long long *nitems,
                          cudaStream_t s);
 

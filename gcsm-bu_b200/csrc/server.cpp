@@ -119,7 +119,6 @@ struct Tenant {
 struct Slot {
     cudaStream_t stream = nullptr;
     EnumScratch sc;
-    uint32_t epoch = 0;
     char *pinned = nullptr;
     uint64_t pinned_bytes = 0;
     std::thread th;
@@ -148,6 +147,7 @@ class Server {
         for (auto &sl : slots_) {
             e = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking);
             if (e == cudaSuccess) e = cudaMalloc(&sl.sc.ctrl, sizeof(EnumControl));
+            if (e == cudaSuccess) e = cudaMemset(sl.sc.ctrl, 0, sizeof(EnumControl));
             if (e == cudaSuccess) e = cudaMalloc(&sl.sc.queue, sizeof(WorkItem) * kSlotQueueItems);
             if (e == cudaSuccess) e = cudaMalloc(&sl.sc.ready, sizeof(uint32_t) * kSlotQueueItems);
             if (e == cudaSuccess) e = cudaMemset(sl.sc.ready, 0, sizeof(uint32_t) * kSlotQueueItems);
@@ -155,7 +155,6 @@ class Server {
             if (e == cudaSuccess) e = cudaMalloc(&sl.sc.ticket_prefix, sizeof(uint32_t) * (kSlotMaxPlans + 1));
             if (e != cudaSuccess) return cuda_fail(e, "slot scratch");
             sl.sc.qcap = kSlotQueueItems;
-            sl.sc.epoch = &sl.epoch;
         }
         for (size_t i = 0; i < slots_.size(); i++) slots_[i].th = std::thread([this, i] { worker(i); });
         started_ = true;

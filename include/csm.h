@@ -75,7 +75,9 @@ typedef struct csm_config {
                                        blocks per SM (fewer registers per thread); 0 = 4 */
     int32_t autotune_batches;       /* >0: over the first batches, time the enumeration under every
                                        candidate launch configuration and keep the fastest */
-    int32_t reserved[3];
+    int32_t cuda_graphs;            /* nonzero: replay each batch's device work from a CUDA graph
+                                       (depth-first strategies 0 and 1; one capture per batch size) */
+    int32_t reserved[2];
 } csm_config;
 
 /* Per-query result of one batch. */
@@ -108,6 +110,8 @@ typedef struct csm_stats {
     uint64_t tuned_steal_chunk;     /* the configured one) */
     uint64_t tuned_warps_per_block;
     uint64_t tuned_occupancy;
+    uint64_t graph_launches;        /* batches replayed from a CUDA graph */
+    uint64_t reserved[3];
 } csm_stats;
 
 /* Fills `cfg` with the defaults (algorithm 0 with all switches on, as main.cpp). */

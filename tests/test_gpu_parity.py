@@ -163,3 +163,37 @@ def test_autotune_keeps_counts_and_reports_choice():
     assert st.tuned_warps_per_block in (4, 8)
     assert st.tuned_occupancy in (4, 5)
     eng.close()
+
+
+@pytest.mark.parametrize("strategy", [0, 1])
+def test_cuda_graph_replay_matches_oracle(strategy):
+    # Batches of two sizes (one capture each, then replays), with deletions.
+    w = small_workload("c2", scale=0.003, batch=1500, nqueries=4)
+    check_stream(w, search_strategy=strategy, cuda_graphs=1)
+    eng = csm.Engine(search_strategy=strategy, cuda_graphs=1)
+    eng.load_query(w.queries[0])
+    eng.load_graph(w.data)
+    for b in w.batches:
+        eng.apply(b)
+    assert eng.stats().graph_launches >= len(w.batches) - 1
+    eng.close()
+
+
+def test_cuda_graph_device_updates_and_autotune():
+    import torch
+    w = small_workload("c2", scale=0.003, batch=1500, nqueries=3)
+    ref = csm.Engine(search_strategy=0)
+    eng = csm.Engine(search_strategy=0, cuda_graphs=1, autotune_batches=1)
+    for e in (ref, eng):
+        for q in w.queries:
+            e.load_query(q)
+        e.load_graph(w.data)
+    for b in list(w.batches) * 2:
+        want = [(r.positive, r.negative) for r in ref.apply(b)]
+        dl = b.is_delete if b.is_delete is not None else np.zeros(len(b.src), dtype=np.uint8)
+        arrs = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in
+                (b.src.astype(np.int32), b.dst.astype(np.int32), b.elabels.astype(np.int32), dl.astype(np.uint8))]
+        got = eng.apply_device(len(b.src), *[a.data_ptr() for a in arrs])
+        assert [(r.positive, r.negative) for r in got] == want
+    ref.close()
+    eng.close()
