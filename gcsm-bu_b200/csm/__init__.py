@@ -36,6 +36,7 @@ ERRORS = {
 # Every symbol declared in include/csm.h.
 EXPORTED = [
     "csm_default_config", "csm_create", "csm_destroy", "csm_load_query", "csm_load_graph",
+    "csm_save_snapshot", "csm_load_snapshot",
     "csm_apply_batch", "csm_apply_batch_device", "csm_apply_batch_device_static", "csm_get_edge_counts", "csm_get_embeddings",
     "csm_free", "csm_describe_plan", "csm_get_stats", "csm_reset_stats", "csm_device_memory",
     "csm_last_error", "csm_version",
@@ -68,7 +69,8 @@ class CsmConfig(ctypes.Structure):
         ("occupancy", ctypes.c_int32),
         ("autotune_batches", ctypes.c_int32),
         ("cuda_graphs", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 2),
+        ("replan_drift_pct", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 1),
     ]
 
 
@@ -90,7 +92,7 @@ class CsmStats(ctypes.Structure):
         "batches", "enum_launches", "kernel_launches", "enum_scan_entries", "enum_probes",
         "enum_tail_lists", "donations", "enum_ns", "apply_ns", "pool_used", "pool_capacity",
         "compactions", "tuned_strategy", "tuned_steal_chunk", "tuned_warps_per_block", "tuned_occupancy",
-        "graph_launches")] + [("reserved", ctypes.c_uint64 * 3)]
+        "graph_launches", "replans")] + [("reserved", ctypes.c_uint64 * 2)]
 
 
 class CsmError(RuntimeError):
@@ -144,6 +146,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.csm_load_query.argtypes = [vp, ctypes.c_uint32, u32p, ctypes.c_uint32, u32p, u32p, u32p,
                                    ctypes.POINTER(ctypes.c_int32)]
     lib.csm_load_graph.argtypes = [vp, ctypes.c_uint32, u32p, ctypes.c_uint64, u32p, u32p, u32p]
+    lib.csm_save_snapshot.argtypes = [vp, ctypes.c_char_p]
+    lib.csm_load_snapshot.argtypes = [vp, ctypes.c_char_p]
     lib.csm_apply_batch.argtypes = [vp, ctypes.c_uint64, u32p, u32p, u32p, u8p, ctypes.POINTER(CsmBatchResult)]
     lib.csm_apply_batch_device.argtypes = [vp, ctypes.c_uint64, vp, vp, vp, vp, vp, ctypes.POINTER(CsmBatchResult)]
     lib.csm_apply_batch_device_static.argtypes = [vp, ctypes.c_uint64, vp, vp, vp, vp, vp,
@@ -270,6 +274,14 @@ class Engine:
     def load_graph(self, g: DataGraph):
         vl, s, d, l = _u32(g.vlabels), _u32(g.src), _u32(g.dst), _u32(g.elabels)
         self._check(self.lib.csm_load_graph(self._h, len(vl), _ptr(vl), len(s), _ptr(s), _ptr(d), _ptr(l)))
+
+    def save_snapshot(self, path: str):
+        """csm_save_snapshot: the data graph after the last batch, to a binary file."""
+        self._check(self.lib.csm_save_snapshot(self._h, os.fsencode(path)))
+
+    def load_snapshot(self, path: str):
+        """csm_load_snapshot: restores a snapshot instead of load_graph (same queries first)."""
+        self._check(self.lib.csm_load_snapshot(self._h, os.fsencode(path)))
 
     def apply(self, b: Batch) -> List[CsmBatchResult]:
         s, d, l = _u32(b.src), _u32(b.dst), _u32(b.elabels)

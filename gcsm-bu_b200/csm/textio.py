@@ -79,3 +79,59 @@ def read_updates(path: str, batch_size: int) -> List[Batch]:
         out.append(Batch(chunk[:, 0].astype(np.uint32), chunk[:, 1].astype(np.uint32), chunk[:, 2].astype(np.uint32),
                          dl if dl.any() else None))
     return out
+
+
+# Binary forms of the data graph and the update stream (read by csmg when a file starts with
+# the magic; no counterpart in the reference, whose text parsing dominates "Read Graphs from
+# Files").  Little-endian:
+#   data:    b"CSMBGRF1", u32 nv, u32 0, u64 ne, u32 vlabel[nv] (0xFFFFFFFF = absent),
+#            u32 src[ne], u32 dst[ne], u32 elabel[ne]
+#   updates: b"CSMBUPD1", u64 n, u32 src[n], u32 dst[n], u32 elabel[n], u8 is_delete[n]
+# Every update record counts as one update line for the batch cut.
+BIN_DATA_MAGIC = b"CSMBGRF1"
+BIN_UPDATE_MAGIC = b"CSMBUPD1"
+
+
+def write_binary_data(path: str, g: DataGraph) -> None:
+    vl = np.ascontiguousarray(g.vlabels, dtype="<u4")
+    with open(path, "wb") as f:
+        f.write(BIN_DATA_MAGIC)
+        f.write(np.array([len(vl), 0], dtype="<u4").tobytes())
+        f.write(np.array([len(g.src)], dtype="<u8").tobytes())
+        for a in (vl, g.src, g.dst, g.elabels):
+            f.write(np.ascontiguousarray(a, dtype="<u4").tobytes())
+
+
+def write_binary_updates(path: str, batches: Sequence[Batch]) -> None:
+    src = np.concatenate([b.src for b in batches]).astype("<u4")
+    dst = np.concatenate([b.dst for b in batches]).astype("<u4")
+    lab = np.concatenate([b.elabels for b in batches]).astype("<u4")
+    dl = np.concatenate([b.is_delete if b.is_delete is not None else np.zeros(len(b.src), dtype=np.uint8)
+                         for b in batches]).astype(np.uint8)
+    with open(path, "wb") as f:
+        f.write(BIN_UPDATE_MAGIC)
+        f.write(np.array([len(src)], dtype="<u8").tobytes())
+        for a in (src, dst, lab, dl):
+            f.write(a.tobytes())
+
+
+def read_binary_data(path: str):
+    with open(path, "rb") as f:
+        if f.read(8) != BIN_DATA_MAGIC:
+            raise ValueError("not a binary data graph")
+        nv, _ = np.frombuffer(f.read(8), dtype="<u4")
+        (ne,) = np.frombuffer(f.read(8), dtype="<u8")
+        arr = np.frombuffer(f.read(4 * (int(nv) + 3 * int(ne))), dtype="<u4")
+    nv, ne = int(nv), int(ne)
+    return arr[:nv], arr[nv: nv + ne], arr[nv + ne: nv + 2 * ne], arr[nv + 2 * ne:]
+
+
+def read_binary_updates(path: str):
+    with open(path, "rb") as f:
+        if f.read(8) != BIN_UPDATE_MAGIC:
+            raise ValueError("not a binary update stream")
+        (n,) = np.frombuffer(f.read(8), dtype="<u8")
+        n = int(n)
+        arr = np.frombuffer(f.read(12 * n), dtype="<u4")
+        dl = np.frombuffer(f.read(n), dtype=np.uint8)
+    return arr[:n], arr[n: 2 * n], arr[2 * n:], dl

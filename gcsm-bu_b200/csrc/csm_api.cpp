@@ -84,6 +84,16 @@ csm_status csm_load_graph(csm_engine *e, uint32_t nv, const uint32_t *vlabel, ui
     return guarded(e, [&] { return e->impl.load_graph(nv, vlabel, ne, src, dst, elabel); });
 }
 
+csm_status csm_save_snapshot(csm_engine *e, const char *path) {
+    if (!e) return CSM_ERR_INVALID_ARG;
+    return guarded(e, [&] { return e->impl.save_snapshot(path); });
+}
+
+csm_status csm_load_snapshot(csm_engine *e, const char *path) {
+    if (!e) return CSM_ERR_INVALID_ARG;
+    return guarded(e, [&] { return e->impl.load_snapshot(path); });
+}
+
 csm_status csm_apply_batch(csm_engine *e, uint64_t n, const uint32_t *src, const uint32_t *dst, const uint32_t *elabel,
                            const uint8_t *is_delete, csm_batch_result *per_query_out) {
     if (!e) return CSM_ERR_INVALID_ARG;

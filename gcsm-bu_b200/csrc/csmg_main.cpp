@@ -109,6 +109,29 @@ bool load_graph_text(const std::string &path, TextGraph &g, bool is_query) {
     return true;
 }
 
+// Binary data graph (magic "CSMBGRF1"): u32 nv, u32 0, u64 ne, u32 vlabel[nv], u32 src[ne],
+// u32 dst[ne], u32 elabel[ne], little-endian.  Returns false if `buf` is not one.
+bool load_graph_binary(const std::string &buf, TextGraph &g, bool &ok) {
+    ok = false;
+    if (buf.size() < 24 || buf.compare(0, 8, "CSMBGRF1") != 0) return false;
+    uint32_t nv = 0;
+    uint64_t ne = 0;
+    std::memcpy(&nv, buf.data() + 8, 4);
+    std::memcpy(&ne, buf.data() + 16, 8);
+    if (buf.size() != 24 + 4ull * nv + 12ull * ne) return true;
+    const char *p = buf.data() + 24;
+    g.vlabel.resize(nv);
+    std::memcpy(g.vlabel.data(), p, 4ull * nv);
+    p += 4ull * nv;
+    for (auto *v : {&g.src, &g.dst, &g.elab}) {
+        v->resize(ne);
+        std::memcpy(v->data(), p, 4 * ne);
+        p += 4 * ne;
+    }
+    ok = true;
+    return true;
+}
+
 void print_info(const Args &args, const std::string &q, const std::string &d, const std::string &u, int32_t dev,
                 uint32_t bs, bool show_mem, const csm_config &cfg) {
     static const char *orders[] = {"BFS Order", "Gamma Order", "RapidCSM Order", "RI Order"};
@@ -187,9 +210,25 @@ int main(int argc, char **argv) {
         std::cout << "Failed to open: " << qpath << std::endl;
         return 255;
     }
-    if (!load_graph_text(dpath, dg, false)) {
-        std::cout << "Failed to open: " << dpath << std::endl;
-        return 255;
+    // Extensions: --snapshot_in restores a device-state checkpoint instead of reading --data;
+    // --snapshot_out writes one after the stream.  Data and update files may be binary.
+    const std::string snap_in = args.get("--snapshot_in"), snap_out = args.get("--snapshot_out");
+    if (snap_in.empty()) {
+        std::string dbuf;
+        if (!read_file(dpath, dbuf)) {
+            std::cout << "Failed to open: " << dpath << std::endl;
+            return 255;
+        }
+        bool bin_ok = false;
+        if (load_graph_binary(dbuf, dg, bin_ok)) {
+            if (!bin_ok) {
+                std::cout << "Corrupt binary data graph: " << dpath << std::endl;
+                return 255;
+            }
+        } else if (!load_graph_text(dpath, dg, false)) {
+            std::cout << "Failed to open: " << dpath << std::endl;
+            return 255;
+        }
     }
     // Update stream: batch k = update lines [k*B, (k+1)*B), counting every update line
     // (graph.cpp:507-516), filtered or not.
@@ -204,7 +243,27 @@ int main(int argc, char **argv) {
         bool any_del = false;
     };
     std::vector<Batch> batches;
-    {
+    if (ubuf.size() >= 16 && ubuf.compare(0, 8, "CSMBUPD1") == 0) {
+        // Binary update stream: u64 n, u32 src[n], u32 dst[n], u32 elabel[n], u8 is_delete[n].
+        uint64_t n = 0;
+        std::memcpy(&n, ubuf.data() + 8, 8);
+        if (ubuf.size() != 16 + 13 * n || batch_size == 0) {
+            std::cout << "Corrupt binary update stream: " << upath << std::endl;
+            return 255;
+        }
+        const uint32_t *us = reinterpret_cast<const uint32_t *>(ubuf.data() + 16);
+        const uint32_t *ud = us + n, *ul = ud + n;
+        const uint8_t *udel = reinterpret_cast<const uint8_t *>(ul + n);
+        for (uint64_t i = 0; i < n; i++) {
+            if (i % batch_size == 0) batches.emplace_back();
+            Batch &bt = batches.back();
+            bt.src.push_back(us[i]);
+            bt.dst.push_back(ud[i]);
+            bt.lab.push_back(ul[i]);
+            bt.del.push_back(udel[i] ? 1 : 0);
+            bt.any_del |= udel[i] != 0;
+        }
+    } else {
         Scanner sc(ubuf);
         std::string w;
         uint64_t a, b, c, nlines = 0;
@@ -249,11 +308,15 @@ int main(int argc, char **argv) {
                        qg.dst.data(), qg.elab.data(), &qid) != CSM_OK)
         return die(e, "query");
     t0 = std::chrono::high_resolution_clock::now();
-    if (csm_load_graph(e, (uint32_t)dg.vlabel.size(), dg.vlabel.data(), dg.src.size(), dg.src.data(), dg.dst.data(),
-                       dg.elab.data()) != CSM_OK)
-        return die(e, "data graph");
+    if (!snap_in.empty()) {
+        if (csm_load_snapshot(e, snap_in.c_str()) != CSM_OK) return die(e, "snapshot");
+    } else {
+        if (csm_load_graph(e, (uint32_t)dg.vlabel.size(), dg.vlabel.data(), dg.src.size(), dg.src.data(),
+                           dg.dst.data(), dg.elab.data()) != CSM_OK)
+            return die(e, "data graph");
+        std::cout << "#data graph vertices: " << dg.vlabel.size() << std::endl;
+    }
     t1 = std::chrono::high_resolution_clock::now();
-    std::cout << "#data graph vertices: " << dg.vlabel.size() << std::endl;
     print_time("Build Global Index Offline", std::chrono::duration<double, std::milli>(t1 - t0).count(), 0);
     {
         std::string plan(1 << 16, '\0');
@@ -296,6 +359,7 @@ int main(int argc, char **argv) {
     std::cout << "--------------------------------------------------------------------" << std::endl;
     std::cout << "Num Positive Matches: " << num_pos << '\n';
     std::cout << "Num Negative Matches: " << num_neg << '\n';
+    if (!snap_out.empty() && csm_save_snapshot(e, snap_out.c_str()) != CSM_OK) return die(e, "snapshot");
     csm_destroy(e);
     return 0;
 }

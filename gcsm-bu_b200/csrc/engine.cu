@@ -2,6 +2,7 @@
 #include "engine.h"
 
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
 #include <map>
 #include <sstream>
@@ -144,7 +145,7 @@ Engine::~Engine() {
                    g_.vlab, d_plans_, d_terms_, d_upd_src_, d_upd_dst_, d_upd_lab_, d_upd_del_, d_keys_raw_, d_keys_,
                    d_sort_temp_, bs_.eff, bs_.heads, bs_.nheads, bs_.seg_nins, bs_.seg_ndel, bs_.seg_end, bs_.scr_y,
                    bs_.scr_lb, bs_.counters, bs_.error, d_ctrl_, d_queue_, d_ready_, d_seed_lo_, d_ticket_prefix_,
-                   d_counts_, d_frontier_[0], d_frontier_[1], d_rows_, d_misc_};
+                   d_counts_, d_frontier_[0], d_frontier_[1], d_rows_, d_misc_, d_rel_delta_};
     for (void *p : dev)
         if (p) cudaFree(p);
     if (h_pin_) cudaFreeHost(h_pin_);
@@ -172,11 +173,22 @@ csm_status Engine::load_query(uint32_t nv, const uint32_t *vlabel, uint32_t ne, 
 
 csm_status Engine::load_graph(uint32_t nv, const uint32_t *vlabel, uint64_t ne, const uint32_t *src,
                               const uint32_t *dst, const uint32_t *elabel) {
-    if (graph_loaded_) return fail(CSM_ERR_STATE, "the data graph is already loaded");
+    if (graph_loaded_ || tables_ready_) return fail(CSM_ERR_STATE, "the data graph is already loaded");
     if (queries_.empty()) return fail(CSM_ERR_STATE, "register at least one query before loading the graph");
     if (nv == 0 || !vlabel) return fail(CSM_ERR_INVALID_ARG, "empty vertex set");
     if (ne && (!src || !dst || !elabel)) return fail(CSM_ERR_INVALID_ARG, "null edge array");
+    csm_status pst = prepare_tables(nv, vlabel, nullptr);
+    if (pst != CSM_OK) return pst;
+    const uint32_t nvl = (uint32_t)vlab_raw_.size(), nel = (uint32_t)elab_raw_.size();
+    return build_lists(ne, src, dst, elabel, nvl, nel);
+}
+
+// Label spaces, relations, candidate-rule specs, key layout and the device tables of a graph
+// of nv vertices (raw vertex labels, or dense labels from a snapshot); allocates the list
+// metadata.
+csm_status Engine::prepare_tables(uint32_t nv, const uint32_t *vlabel, const uint8_t *vlab_dense) {
     CSM_CUDA(cudaSetDevice(device_));
+    tables_ready_ = true;
     // Label spaces: the union of the labels of all queries (graph.cpp:389-433 keeps only
     // data labels that occur in the query).
     for (auto &q : queries_) {
@@ -244,9 +256,14 @@ csm_status Engine::load_graph(uint32_t nv, const uint32_t *vlabel, uint64_t ne, 
 
     // Dense vertex labels.
     std::vector<uint8_t> vlab(nv, CSM_NO_LABEL);
-    for (uint32_t v = 0; v < nv; v++) {
-        auto it = std::lower_bound(vlab_raw_.begin(), vlab_raw_.end(), vlabel[v]);
-        if (it != vlab_raw_.end() && *it == vlabel[v]) vlab[v] = (uint8_t)(it - vlab_raw_.begin());
+    if (vlab_dense) {
+        for (uint32_t v = 0; v < nv; v++)
+            vlab[v] = vlab_dense[v] < nvl ? vlab_dense[v] : (uint8_t)CSM_NO_LABEL;
+    } else {
+        for (uint32_t v = 0; v < nv; v++) {
+            auto it = std::lower_bound(vlab_raw_.begin(), vlab_raw_.end(), vlabel[v]);
+            if (it != vlab_raw_.end() && *it == vlabel[v]) vlab[v] = (uint8_t)(it - vlab_raw_.begin());
+        }
     }
     const size_t nmeta = (size_t)g_.R * nv;
     CSM_CUDA(dalloc(&g_.vlab, nv));
@@ -265,7 +282,12 @@ csm_status Engine::load_graph(uint32_t nv, const uint32_t *vlabel, uint64_t ne, 
     CSM_CUDA(dalloc(&g_.meta, nmeta));
     CSM_CUDA(dalloc(&g_.cap, nmeta));
     CSM_CUDA(dalloc(&g_.pool_top, 1));
+    return CSM_OK;
+}
 
+// Initial lists from edge arrays, then the rest of the load.
+csm_status Engine::build_lists(uint64_t ne, const uint32_t *src, const uint32_t *dst, const uint32_t *elabel,
+                               uint32_t nvl, uint32_t nel) {
     // Edges -> keys -> sorted -> lists.
     const uint64_t m64 = 2 * ne;
     if (m64 >= 0x7FFFFFFFull) return fail(CSM_ERR_LIMIT, "too many initial edges for one load (limit 2^30)");
@@ -324,59 +346,34 @@ csm_status Engine::load_graph(uint32_t nv, const uint32_t *vlabel, uint64_t ne, 
     cudaFree(k_sorted);
     cudaFree(temp);
     if (st != CSM_OK) return st;
+    return finish_load();
+}
 
+// Candidate bitmaps, planner statistics, plans and the per-batch buffers of a loaded graph.
+csm_status Engine::finish_load() {
     // Candidate bitmaps, planner statistics, plans.
     NlfTables nt{d_spec_begin_, d_specs_, d_bits_, words_};
     store_nlf_all(g_, nt, stream_);
-    unsigned long long *d_stat = nullptr;
-    CSM_CUDA(dalloc(&d_stat, 2));
-    std::vector<EdgeStats> stats(queries_.size());
-    for (size_t qi = 0; qi < queries_.size(); qi++) {
-        const Query &q = queries_[qi];
-        stats[qi].card.assign(q.nv * q.nv, 0);
-        stats[qi].avg.assign(q.nv * q.nv, 0.f);
-        for (uint32_t u = 0; u < q.nv; u++)
-            for (auto &p : q.nbrs[u]) {
-                const uint32_t uu = p.first;
-                const uint16_t rel = rel_table_[((size_t)vl(q.vlabel[u]) * nel + el(p.second)) * nvl + vl(q.vlabel[uu])];
-                CSM_CUDA(cudaMemsetAsync(d_stat, 0, 16, stream_));
-                store_edge_stats(g_, rel, d_bits_ + (size_t)(nlf_base_[qi] + u) * words_,
-                                 d_bits_ + (size_t)(nlf_base_[qi] + uu) * words_, d_stat, stream_);
-                unsigned long long h[2];
-                CSM_CUDA(cudaMemcpyAsync(h, d_stat, 16, cudaMemcpyDeviceToHost, stream_));
-                CSM_CUDA(cudaStreamSynchronize(stream_));
-                stats[qi].card[u * q.nv + uu] = (uint32_t)std::min<unsigned long long>(h[0], 0xFFFFFFFFull);
-                // GetSummary divides by the number of sources (match_gpu.cu:607), NaN when empty.
-                stats[qi].avg[u * q.nv + uu] = (float)h[0] / (float)h[1];
-            }
+    std::vector<EdgeStats> stats;
+    csm_status pst = compute_edge_stats(stats);
+    if (pst != CSM_OK) return pst;
+    pst = install_plans(stats);
+    if (pst != CSM_OK) return pst;
+    if (cfg_.replan_drift_pct > 0) {
+        // Relation sizes at planning time, for the drift check after each batch.
+        unsigned long long *d_sz = nullptr;
+        CSM_CUDA(dalloc(&d_sz, g_.R));
+        CSM_CUDA(cudaMemsetAsync(d_sz, 0, sizeof(unsigned long long) * g_.R, stream_));
+        store_rel_sizes(g_, d_sz, stream_);
+        std::vector<unsigned long long> h(g_.R);
+        CSM_CUDA(cudaMemcpyAsync(h.data(), d_sz, sizeof(unsigned long long) * g_.R, cudaMemcpyDeviceToHost, stream_));
+        CSM_CUDA(cudaStreamSynchronize(stream_));
+        cudaFree(d_sz);
+        rel_size_.assign(h.begin(), h.end());
+        rel_size_planned_ = rel_size_;
+        CSM_CUDA(dalloc(&d_rel_delta_, g_.R));
+        CSM_CUDA(cudaMallocHost(&h_rel_delta_, sizeof(long long) * g_.R));
     }
-    cudaFree(d_stat);
-    for (size_t qi = 0; qi < queries_.size(); qi++) {
-        const Query &q = queries_[qi];
-        PlanOptions po;
-        po.order = opt_.order;
-        po.cartesian = opt_.cartesian;
-        po.materialize = cfg_.materialize_rows > 0;
-        auto rel_of = [&](uint32_t u, uint32_t uu) -> uint16_t {
-            return rel_table_[((size_t)vl(q.vlabel[u]) * nel + el(q.edge_label(u, uu))) * nvl + vl(q.vlabel[uu])];
-        };
-        auto ps = build_plans(q, (uint16_t)qi, nlf_base_[qi], stats[qi], po, rel_of);
-        plan_begin_.push_back((uint32_t)plans_.size());
-        plans_.insert(plans_.end(), ps.begin(), ps.end());
-    }
-    plan_begin_.push_back((uint32_t)plans_.size());
-    std::vector<DevPlan> dplans;
-    std::vector<DevTailTerm> terms;
-    for (auto &hp : plans_) {
-        hp.dev.term_begin = (uint32_t)terms.size();
-        terms.insert(terms.end(), hp.terms.begin(), hp.terms.end());
-        dplans.push_back(hp.dev);
-    }
-    CSM_CUDA(dalloc(&d_plans_, dplans.size()));
-    CSM_CUDA(cudaMemcpy(d_plans_, dplans.data(), sizeof(DevPlan) * dplans.size(), cudaMemcpyHostToDevice));
-    CSM_CUDA(dalloc(&d_terms_, terms.size()));
-    if (!terms.empty())
-        CSM_CUDA(cudaMemcpy(d_terms_, terms.data(), sizeof(DevTailTerm) * terms.size(), cudaMemcpyHostToDevice));
     const uint32_t np = (uint32_t)plans_.size();
     CSM_CUDA(dalloc(&d_seed_lo_, 3 * (size_t)np));
     CSM_CUDA(dalloc(&d_ticket_prefix_, np + 1));
@@ -416,6 +413,243 @@ csm_status Engine::load_graph(uint32_t nv, const uint32_t *vlabel, uint64_t ne, 
     stats_.pool_capacity = g_.pool_cap;
     graph_loaded_ = true;
     return CSM_OK;
+}
+
+// Planner statistics per directed query edge: candidate edges between the two endpoints'
+// candidate sets and the average over sources (GetSummary, match_gpu.cu:589-609).
+csm_status Engine::compute_edge_stats(std::vector<EdgeStats> &stats) {
+    const uint32_t nvl = (uint32_t)vlab_raw_.size(), nel = (uint32_t)elab_raw_.size();
+    auto vl = [&](uint32_t raw) {
+        return (uint32_t)(std::lower_bound(vlab_raw_.begin(), vlab_raw_.end(), raw) - vlab_raw_.begin());
+    };
+    auto el = [&](uint32_t raw) {
+        return (uint32_t)(std::lower_bound(elab_raw_.begin(), elab_raw_.end(), raw) - elab_raw_.begin());
+    };
+    unsigned long long *d_stat = nullptr;
+    CSM_CUDA(dalloc(&d_stat, 2));
+    stats.assign(queries_.size(), EdgeStats{});
+    for (size_t qi = 0; qi < queries_.size(); qi++) {
+        const Query &q = queries_[qi];
+        stats[qi].card.assign(q.nv * q.nv, 0);
+        stats[qi].avg.assign(q.nv * q.nv, 0.f);
+        for (uint32_t u = 0; u < q.nv; u++)
+            for (auto &p : q.nbrs[u]) {
+                const uint32_t uu = p.first;
+                const uint16_t rel = rel_table_[((size_t)vl(q.vlabel[u]) * nel + el(p.second)) * nvl + vl(q.vlabel[uu])];
+                CSM_CUDA(cudaMemsetAsync(d_stat, 0, 16, stream_));
+                store_edge_stats(g_, rel, d_bits_ + (size_t)(nlf_base_[qi] + u) * words_,
+                                 d_bits_ + (size_t)(nlf_base_[qi] + uu) * words_, d_stat, stream_);
+                unsigned long long h[2];
+                CSM_CUDA(cudaMemcpyAsync(h, d_stat, 16, cudaMemcpyDeviceToHost, stream_));
+                CSM_CUDA(cudaStreamSynchronize(stream_));
+                stats[qi].card[u * q.nv + uu] = (uint32_t)std::min<unsigned long long>(h[0], 0xFFFFFFFFull);
+                // GetSummary divides by the number of sources (match_gpu.cu:607), NaN when empty.
+                stats[qi].avg[u * q.nv + uu] = (float)h[0] / (float)h[1];
+            }
+    }
+    cudaFree(d_stat);
+    return CSM_OK;
+}
+
+// Builds every query's plans from the statistics and uploads them (the plan count per query
+// never changes; the tail-term array is regrown when a new plan set needs more terms).
+csm_status Engine::install_plans(const std::vector<EdgeStats> &stats) {
+    const uint32_t nvl = (uint32_t)vlab_raw_.size(), nel = (uint32_t)elab_raw_.size();
+    auto vl = [&](uint32_t raw) {
+        return (uint32_t)(std::lower_bound(vlab_raw_.begin(), vlab_raw_.end(), raw) - vlab_raw_.begin());
+    };
+    auto el = [&](uint32_t raw) {
+        return (uint32_t)(std::lower_bound(elab_raw_.begin(), elab_raw_.end(), raw) - elab_raw_.begin());
+    };
+    std::vector<HostPlan> plans;
+    std::vector<uint32_t> begin;
+    for (size_t qi = 0; qi < queries_.size(); qi++) {
+        const Query &q = queries_[qi];
+        PlanOptions po;
+        po.order = opt_.order;
+        po.cartesian = opt_.cartesian;
+        po.materialize = cfg_.materialize_rows > 0;
+        auto rel_of = [&](uint32_t u, uint32_t uu) -> uint16_t {
+            return rel_table_[((size_t)vl(q.vlabel[u]) * nel + el(q.edge_label(u, uu))) * nvl + vl(q.vlabel[uu])];
+        };
+        auto ps = build_plans(q, (uint16_t)qi, nlf_base_[qi], stats[qi], po, rel_of);
+        begin.push_back((uint32_t)plans.size());
+        plans.insert(plans.end(), ps.begin(), ps.end());
+    }
+    begin.push_back((uint32_t)plans.size());
+    if (!plans_.empty() && plans.size() != plans_.size()) return fail(CSM_ERR_STATE, "re-planning changed the plan count");
+    std::vector<DevPlan> dplans;
+    std::vector<DevTailTerm> terms;
+    for (auto &hp : plans) {
+        hp.dev.term_begin = (uint32_t)terms.size();
+        terms.insert(terms.end(), hp.terms.begin(), hp.terms.end());
+        dplans.push_back(hp.dev);
+    }
+    if (!d_plans_) CSM_CUDA(dalloc(&d_plans_, dplans.size()));
+    CSM_CUDA(cudaMemcpyAsync(d_plans_, dplans.data(), sizeof(DevPlan) * dplans.size(), cudaMemcpyHostToDevice, stream_));
+    if (terms.size() > terms_cap_ || !d_terms_) {
+        if (d_terms_) cudaFree(d_terms_);
+        d_terms_ = nullptr;
+        terms_cap_ = std::max<size_t>(terms.size(), 1);
+        CSM_CUDA(dalloc(&d_terms_, terms_cap_));
+    }
+    if (!terms.empty())
+        CSM_CUDA(cudaMemcpyAsync(d_terms_, terms.data(), sizeof(DevTailTerm) * terms.size(), cudaMemcpyHostToDevice,
+                                 stream_));
+    CSM_CUDA(cudaStreamSynchronize(stream_));
+    plans_ = std::move(plans);
+    plan_begin_ = std::move(begin);
+    return CSM_OK;
+}
+
+// Re-plans when a relation the plans read has grown or shrunk by more than the configured
+// fraction since the plans were made (the reference plans once, technique_permutation.h:91-107).
+csm_status Engine::maybe_replan() {
+    bool drift = false;
+    for (uint32_t r = 0; r < g_.R; r++) {
+        rel_size_[r] += h_rel_delta_[r];
+        const long long base = std::max<long long>(rel_size_planned_[r], 1024);
+        const long long diff = rel_size_[r] - rel_size_planned_[r];
+        if ((diff < 0 ? -diff : diff) * 100 > (long long)cfg_.replan_drift_pct * base) drift = true;
+    }
+    if (!drift) return CSM_OK;
+    std::vector<EdgeStats> stats;
+    csm_status st = compute_edge_stats(stats);
+    if (st != CSM_OK) return st;
+    st = install_plans(stats);
+    if (st != CSM_OK) return st;
+    rel_size_planned_ = rel_size_;
+    clear_graphs();
+    graph_gen_++;
+    stats_.replans++;
+    return CSM_OK;
+}
+
+// ---- Snapshots --------------------------------------------------------------------------
+// File layout (little-endian): "CSMSNAP1", u32 version, u32 V, u32 R, u32 nqueries,
+// u64 query fingerprint, u64 pool entries in use, u64 pool capacity, u8 dense vertex label[V],
+// uint2 meta[R*V] (offset, size), u32 cap[R*V], u32 pool[in use].  Candidate bitmaps, plans and
+// batch buffers are rebuilt on load; the lists keep their slack and layout.
+
+namespace {
+constexpr char kSnapMagic[8] = {'C', 'S', 'M', 'S', 'N', 'A', 'P', '1'};
+constexpr uint32_t kSnapVersion = 1;
+
+struct SnapHeader {
+    char magic[8];
+    uint32_t version, V, R, nqueries;
+    uint64_t fingerprint, used, capacity;
+};
+
+struct FileCloser {
+    FILE *f;
+    ~FileCloser() {
+        if (f) std::fclose(f);
+    }
+};
+}  // namespace
+
+// FNV-1a over every query's vertex labels and labelled adjacency, in registration order: equal
+// fingerprints mean equal relation numbering and list layout.
+uint64_t Engine::query_fingerprint() const {
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&](uint32_t x) {
+        for (int i = 0; i < 4; i++) {
+            h ^= (x >> (8 * i)) & 0xFFu;
+            h *= 1099511628211ull;
+        }
+    };
+    mix((uint32_t)queries_.size());
+    for (auto &q : queries_) {
+        mix(q.nv);
+        for (uint32_t u = 0; u < q.nv; u++) {
+            mix(q.vlabel[u]);
+            mix((uint32_t)q.nbrs[u].size());
+            for (auto &p : q.nbrs[u]) {
+                mix(p.first);
+                mix(p.second);
+            }
+        }
+    }
+    return h;
+}
+
+csm_status Engine::save_snapshot(const char *path) {
+    if (!path) return fail(CSM_ERR_INVALID_ARG, "null path");
+    if (!graph_loaded_) return fail(CSM_ERR_STATE, "load the data graph first");
+    if (poisoned_) return fail(CSM_ERR_STATE, "the engine failed an earlier batch; recreate it");
+    CSM_CUDA(cudaSetDevice(device_));
+    CSM_CUDA(cudaStreamSynchronize(stream_));
+    unsigned long long used = 0;
+    CSM_CUDA(cudaMemcpy(&used, g_.pool_top, sizeof(used), cudaMemcpyDeviceToHost));
+    const size_t nmeta = (size_t)g_.R * g_.V;
+    std::vector<uint8_t> vlab(g_.V);
+    std::vector<uint2> meta(nmeta);
+    std::vector<uint32_t> cap(nmeta), pool(used);
+    CSM_CUDA(cudaMemcpy(vlab.data(), g_.vlab, g_.V, cudaMemcpyDeviceToHost));
+    CSM_CUDA(cudaMemcpy(meta.data(), g_.meta, sizeof(uint2) * nmeta, cudaMemcpyDeviceToHost));
+    CSM_CUDA(cudaMemcpy(cap.data(), g_.cap, sizeof(uint32_t) * nmeta, cudaMemcpyDeviceToHost));
+    if (used) CSM_CUDA(cudaMemcpy(pool.data(), g_.pool, sizeof(uint32_t) * used, cudaMemcpyDeviceToHost));
+    SnapHeader h{};
+    std::memcpy(h.magic, kSnapMagic, 8);
+    h.version = kSnapVersion;
+    h.V = g_.V;
+    h.R = g_.R;
+    h.nqueries = (uint32_t)queries_.size();
+    h.fingerprint = query_fingerprint();
+    h.used = used;
+    h.capacity = g_.pool_cap;
+    FileCloser fc{std::fopen(path, "wb")};
+    if (!fc.f) return fail(CSM_ERR_INVALID_ARG, std::string("cannot create ") + path);
+    bool ok = std::fwrite(&h, sizeof(h), 1, fc.f) == 1 && std::fwrite(vlab.data(), 1, vlab.size(), fc.f) == vlab.size() &&
+              std::fwrite(meta.data(), sizeof(uint2), nmeta, fc.f) == nmeta &&
+              std::fwrite(cap.data(), sizeof(uint32_t), nmeta, fc.f) == nmeta &&
+              std::fwrite(pool.data(), sizeof(uint32_t), used, fc.f) == used;
+    ok = std::fflush(fc.f) == 0 && ok;
+    if (!ok) return fail(CSM_ERR_INVALID_ARG, std::string("write failed: ") + path);
+    return CSM_OK;
+}
+
+csm_status Engine::load_snapshot(const char *path) {
+    if (!path) return fail(CSM_ERR_INVALID_ARG, "null path");
+    if (graph_loaded_ || tables_ready_) return fail(CSM_ERR_STATE, "the data graph is already loaded");
+    if (queries_.empty()) return fail(CSM_ERR_STATE, "register the snapshot's queries before loading it");
+    FileCloser fc{std::fopen(path, "rb")};
+    if (!fc.f) return fail(CSM_ERR_INVALID_ARG, std::string("cannot open ") + path);
+    SnapHeader h{};
+    if (std::fread(&h, sizeof(h), 1, fc.f) != 1 || std::memcmp(h.magic, kSnapMagic, 8) != 0 || h.version != kSnapVersion)
+        return fail(CSM_ERR_INVALID_ARG, "not a snapshot of this format");
+    if (h.nqueries != queries_.size() || h.fingerprint != query_fingerprint())
+        return fail(CSM_ERR_INVALID_ARG, "the snapshot was taken with other queries");
+    if (h.V == 0 || h.used > h.capacity || h.capacity > 0xFFFFFFF0ull)
+        return fail(CSM_ERR_INVALID_ARG, "corrupt snapshot header");
+    std::vector<uint8_t> vlab(h.V);
+    if (std::fread(vlab.data(), 1, h.V, fc.f) != h.V) return fail(CSM_ERR_INVALID_ARG, "truncated snapshot");
+    csm_status st = prepare_tables(h.V, nullptr, vlab.data());
+    if (st != CSM_OK) return st;
+    if (g_.R != h.R) return fail(CSM_ERR_INVALID_ARG, "the snapshot's relations differ from the queries'");
+    const size_t nmeta = (size_t)g_.R * g_.V;
+    std::vector<uint2> meta(nmeta);
+    std::vector<uint32_t> cap(nmeta), pool(h.used);
+    if (std::fread(meta.data(), sizeof(uint2), nmeta, fc.f) != nmeta ||
+        std::fread(cap.data(), sizeof(uint32_t), nmeta, fc.f) != nmeta ||
+        std::fread(pool.data(), sizeof(uint32_t), h.used, fc.f) != h.used)
+        return fail(CSM_ERR_INVALID_ARG, "truncated snapshot");
+    for (size_t i = 0; i < nmeta; i++)
+        if ((uint64_t)meta[i].x + cap[i] > h.used || meta[i].y > cap[i])
+            return fail(CSM_ERR_INVALID_ARG, "corrupt snapshot list table");
+    const uint64_t max_batch = cfg_.max_batch ? cfg_.max_batch : (1ull << 20);
+    unsigned long long want = cfg_.pool_entries ? cfg_.pool_entries : h.capacity;
+    want = std::max<unsigned long long>(want, h.used + 64 * max_batch + (1u << 20));
+    if (want > 0xFFFFFFF0ull) want = 0xFFFFFFF0ull;
+    g_.pool_cap = want;
+    CSM_CUDA(dalloc(&g_.pool, g_.pool_cap));
+    CSM_CUDA(cudaMemcpy(g_.meta, meta.data(), sizeof(uint2) * nmeta, cudaMemcpyHostToDevice));
+    CSM_CUDA(cudaMemcpy(g_.cap, cap.data(), sizeof(uint32_t) * nmeta, cudaMemcpyHostToDevice));
+    if (h.used) CSM_CUDA(cudaMemcpy(g_.pool, pool.data(), sizeof(uint32_t) * h.used, cudaMemcpyHostToDevice));
+    const unsigned long long top = h.used;
+    CSM_CUDA(cudaMemcpy(g_.pool_top, &top, sizeof(top), cudaMemcpyHostToDevice));
+    return finish_load();
 }
 
 csm_status Engine::ensure_batch_capacity(uint64_t n) {
@@ -560,6 +794,11 @@ csm_status Engine::enqueue_batch(uint64_t n, const uint32_t *src, const uint32_t
         CSM_CUDA(store_sort_keys(d_sort_temp_, tb, d_keys_raw_, d_keys_, m, kl_, s));
         store_classify(m, d_keys_, kl_, g_, bs_, s);
         stats_.kernel_launches += 3;
+        if (d_rel_delta_) {
+            CSM_CUDA(cudaMemsetAsync(d_rel_delta_, 0, sizeof(long long) * g_.R, s));
+            store_rel_delta(m, d_keys_, kl_, bs_, d_rel_delta_, s);
+            stats_.kernel_launches++;
+        }
         if (has_delete) {
             // Destroyed embeddings are counted on the graph before the deletions, with the
             // deleted edges flagged; then the flagged entries are compacted away.
@@ -608,6 +847,8 @@ csm_status Engine::enqueue_readback(cudaStream_t s) {
     CSM_CUDA(cudaMemcpyAsync(h_counts_ + 2 * np + 2, g_.pool_top, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                              s));
     CSM_CUDA(cudaMemcpyAsync(h_err, bs_.error, sizeof(unsigned int), cudaMemcpyDeviceToHost, s));
+    if (d_rel_delta_)
+        CSM_CUDA(cudaMemcpyAsync(h_rel_delta_, d_rel_delta_, sizeof(long long) * g_.R, cudaMemcpyDeviceToHost, s));
     return CSM_OK;
 }
 
@@ -756,7 +997,12 @@ csm_status Engine::run_batch(uint64_t n, const uint32_t *src, const uint32_t *ds
         }
     }
     if (cfg_.materialize_rows) rows_valid_ = true;
-    return no_alloc_ ? CSM_OK : maybe_compact(s);
+    if (no_alloc_) return CSM_OK;
+    if (d_rel_delta_ && m) {
+        const csm_status rst = maybe_replan();
+        if (rst != CSM_OK) return rst;
+    }
+    return maybe_compact(s);
 }
 
 csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {

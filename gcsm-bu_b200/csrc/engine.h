@@ -69,6 +69,10 @@ class Engine {
                           const uint32_t *elabel, int32_t *qid);
     csm_status load_graph(uint32_t nv, const uint32_t *vlabel, uint64_t ne, const uint32_t *src, const uint32_t *dst,
                           const uint32_t *elabel);
+    // Device-state checkpoint of the data graph (lists with their slack); load_snapshot replaces
+    // load_graph in an engine with the same registered queries.
+    csm_status save_snapshot(const char *path);
+    csm_status load_snapshot(const char *path);
     csm_status apply_host(uint64_t n, const uint32_t *src, const uint32_t *dst, const uint32_t *elabel,
                           const uint8_t *is_delete, csm_batch_result *out);
     csm_status apply_device(uint64_t n, const uint32_t *src, const uint32_t *dst, const uint32_t *elabel,
@@ -193,6 +197,20 @@ class Engine {
     csm_status enqueue_batch(uint64_t n, const uint32_t *src, const uint32_t *dst, const uint32_t *elabel,
                              const uint8_t *is_delete, bool has_delete, bool tuning, cudaStream_t s);
     csm_status enqueue_readback(cudaStream_t s);
+    // Live re-planning: planner statistics, plan upload, and the drift check after a batch.
+    csm_status prepare_tables(uint32_t nv, const uint32_t *vlabel, const uint8_t *vlab_dense);
+    csm_status build_lists(uint64_t ne, const uint32_t *src, const uint32_t *dst, const uint32_t *elabel, uint32_t nvl,
+                           uint32_t nel);
+    csm_status finish_load();
+    uint64_t query_fingerprint() const;
+    bool tables_ready_ = false;
+    csm_status compute_edge_stats(std::vector<EdgeStats> &stats);
+    csm_status install_plans(const std::vector<EdgeStats> &stats);
+    csm_status maybe_replan();
+    size_t terms_cap_ = 0;
+    long long *d_rel_delta_ = nullptr;      // [R] net entry change of the current batch
+    long long *h_rel_delta_ = nullptr;      // pinned copy
+    std::vector<long long> rel_size_, rel_size_planned_;
     csm_status launch_graph(uint64_t n, bool has_delete, cudaStream_t s);
     void clear_graphs();
     csm_status apply_host_on(cudaStream_t s, uint64_t n, const uint32_t *src, const uint32_t *dst,

@@ -405,6 +405,41 @@ __global__ void k_edge_stats(uint32_t V, const uint2 *meta, const uint32_t *pool
     if (srcs) atomicAdd(out + 1, srcs);
 }
 
+// Net change of each relation's entry count in this batch (+1 per effective insertion, -1 per
+// effective deletion, per key orientation).  Keys are sorted by relation, so the lanes of a warp
+// mostly share one relation: each group of equal relations adds its sum once.
+__global__ void k_rel_delta(uint32_t m, const unsigned long long *keys, KeyLayout kl, const uint8_t *eff,
+                            long long *delta) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool in = i < m;
+    const uint32_t rel = in ? kl.rel(keys[i]) : 0xFFFFFFFFu;
+    const uint8_t e = in ? eff[i] : CSM_EFF_NONE;
+    int v = e == CSM_EFF_INS ? 1 : (e == CSM_EFF_DEL ? -1 : 0);
+    const uint32_t group = __match_any_sync(0xffffffffu, rel);
+    int sum = 0;
+    for (uint32_t g = group; g; g &= g - 1) sum += __shfl_sync(group, v, __ffs(g) - 1);
+    if (in && sum != 0 && (threadIdx.x & 31u) == (uint32_t)(__ffs(group) - 1))
+        atomicAdd(reinterpret_cast<unsigned long long *>(delta + rel), (unsigned long long)(long long)sum);  // two's complement
+}
+
+// Entry count of every relation (sum of its list sizes).  The loop is warp-uniform so that all
+// lanes take part in the grouping shuffles.
+__global__ void k_rel_sizes(uint32_t V, uint32_t R, const uint2 *meta, unsigned long long *out) {
+    const size_t total = (size_t)V * R;
+    const uint32_t lane = threadIdx.x & 31u;
+    const size_t warps = (size_t)gridDim.x * (blockDim.x >> 5);
+    for (size_t w = (size_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); w * 32 < total; w += warps) {
+        const size_t i = w * 32 + lane;
+        const bool in = i < total;
+        const uint32_t rel = in ? (uint32_t)(i / V) : 0xFFFFFFFFu;
+        const uint32_t sz = in ? meta[i].y : 0u;
+        const uint32_t group = __match_any_sync(0xffffffffu, rel);
+        unsigned long long sum = 0;
+        for (uint32_t g = group; g; g &= g - 1) sum += __shfl_sync(group, sz, __ffs(g) - 1);
+        if (in && lane == (uint32_t)(__ffs(group) - 1) && sum) atomicAdd(out + rel, sum);
+    }
+}
+
 inline int grid_for(size_t n, int block) {
     size_t g = (n + block - 1) / block;
     if (g < 1) g = 1;
@@ -461,6 +496,15 @@ void store_clear_ins(uint32_t m, const unsigned long long *keys, KeyLayout kl, D
 
 void store_nlf_all(DeviceGraph &g, const NlfTables &nt, cudaStream_t s) {
     k_nlf_all<<<grid_for(g.V, 256), 256, 0, s>>>(g.V, g.vlab, g.meta, nt.spec_begin, nt.specs, nt.bits, nt.words);
+}
+
+void store_rel_delta(uint32_t m, const unsigned long long *keys, KeyLayout kl, const BatchScratch &b, long long *delta,
+                     cudaStream_t s) {
+    if (m) k_rel_delta<<<(m + 255) / 256, 256, 0, s>>>(m, keys, kl, b.eff, delta);
+}
+
+void store_rel_sizes(const DeviceGraph &g, unsigned long long *out, cudaStream_t s) {
+    k_rel_sizes<<<grid_for((size_t)g.V * g.R, 256), 256, 0, s>>>(g.V, g.R, g.meta, out);
 }
 
 void store_edge_stats(DeviceGraph &g, uint32_t rel, const uint32_t *bits_u, const uint32_t *bits_uu,

@@ -76,6 +76,11 @@ void store_nlf_update(uint32_t m, const unsigned long long *keys, KeyLayout kl, 
 void store_clear_ins(uint32_t m, const unsigned long long *keys, KeyLayout kl, DeviceGraph &g, BatchScratch &b,
                      cudaStream_t s);
 void store_nlf_all(DeviceGraph &g, const NlfTables &nt, cudaStream_t s);
+// Per-relation net entry change of a classified batch (delta[R], accumulated).
+void store_rel_delta(uint32_t m, const unsigned long long *keys, KeyLayout kl, const BatchScratch &b, long long *delta,
+                     cudaStream_t s);
+// Per-relation entry counts (out[R], accumulated).
+void store_rel_sizes(const DeviceGraph &g, unsigned long long *out, cudaStream_t s);
 void store_edge_stats(DeviceGraph &g, uint32_t rel, const uint32_t *bits_u, const uint32_t *bits_uu,
                       unsigned long long *out, cudaStream_t s);
 cudaError_t store_build_from_keys(DeviceGraph &g, const unsigned long long *keys_sorted, uint32_t m, KeyLayout kl,

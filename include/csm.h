@@ -77,7 +77,10 @@ typedef struct csm_config {
                                        candidate launch configuration and keep the fastest */
     int32_t cuda_graphs;            /* nonzero: replay each batch's device work from a CUDA graph
                                        (depth-first strategies 0 and 1; one capture per batch size) */
-    int32_t reserved[2];
+    int32_t replan_drift_pct;       /* >0: re-plan the matching orders after a batch that moved a
+                                       relation's size by more than this percentage since the last
+                                       planning (the reference plans once, before the stream) */
+    int32_t reserved[1];
 } csm_config;
 
 /* Per-query result of one batch. */
@@ -111,7 +114,8 @@ typedef struct csm_stats {
     uint64_t tuned_warps_per_block;
     uint64_t tuned_occupancy;
     uint64_t graph_launches;        /* batches replayed from a CUDA graph */
-    uint64_t reserved[3];
+    uint64_t replans;               /* re-plannings triggered by relation-size drift */
+    uint64_t reserved[2];
 } csm_stats;
 
 /* Fills `cfg` with the defaults (algorithm 0 with all switches on, as main.cpp). */
@@ -142,6 +146,17 @@ csm_status csm_load_query(csm_engine *engine, uint32_t nv, const uint32_t *vlabe
  */
 csm_status csm_load_graph(csm_engine *engine, uint32_t nv, const uint32_t *vlabel, uint64_t ne,
                           const uint32_t *src, const uint32_t *dst, const uint32_t *elabel);
+
+/*
+ * Device-state checkpoint (no counterpart in the reference, which re-reads and re-indexes its
+ * text files on every start, technique_permutation.h:28-107).  csm_save_snapshot writes the
+ * data graph as it stands after the last completed batch — the label-partitioned adjacency
+ * lists with their slack — to a binary file.  csm_load_snapshot takes the place of
+ * csm_load_graph in an engine whose registered queries are the same (checked by fingerprint);
+ * candidate bitmaps and plans are rebuilt from the restored lists.
+ */
+csm_status csm_save_snapshot(csm_engine *engine, const char *path);
+csm_status csm_load_snapshot(csm_engine *engine, const char *path);
 
 /*
  * Applies one update batch and counts its incremental matches for every registered query.

@@ -197,3 +197,51 @@ def test_cuda_graph_device_updates_and_autotune():
         assert [(r.positive, r.negative) for r in got] == want
     ref.close()
     eng.close()
+
+
+@pytest.mark.parametrize("graphs", [0, 1])
+def test_live_replanning_keeps_counts(graphs):
+    # A 1% drift threshold re-plans after nearly every batch; the counts must not change.
+    w = small_workload("c2", scale=0.003, batch=1500, nqueries=4)
+    check_stream(w, replan_drift_pct=1, cuda_graphs=graphs, search_strategy=0 if graphs else 2)
+    eng = csm.Engine(replan_drift_pct=1)
+    for q in w.queries:
+        eng.load_query(q)
+    eng.load_graph(w.data)
+    for b in w.batches:
+        eng.apply(b)
+    assert eng.stats().replans >= 1
+    eng.close()
+
+
+def test_snapshot_restore_continues_stream(tmp_path):
+    w = small_workload("c2", scale=0.003, batch=1500, nqueries=3)
+    a = csm.Engine()
+    for q in w.queries:
+        a.load_query(q)
+    a.load_graph(w.data)
+    half = len(w.batches) // 2
+    for b in w.batches[:half]:
+        a.apply(b)
+    snap = str(tmp_path / "state.snap")
+    a.save_snapshot(snap)
+    b_eng = csm.Engine(search_strategy=0)
+    for q in w.queries:
+        b_eng.load_query(q)
+    b_eng.load_snapshot(snap)
+    oracles = [Oracle(q, w.data) for q in w.queries]
+    for bt in w.batches[:half]:
+        for o in oracles:
+            o.apply(bt)
+    for bt in w.batches[half:]:
+        ra = [(r.positive, r.negative) for r in a.apply(bt)]
+        rb = [(r.positive, r.negative) for r in b_eng.apply(bt)]
+        ro = [(x["pos"], x["neg"]) for x in (o.apply(bt) for o in oracles)]
+        assert ra == rb == ro
+    # A snapshot is refused by an engine with other queries.
+    c = csm.Engine()
+    c.load_query(w.queries[0])
+    with pytest.raises(csm.CsmError):
+        c.load_snapshot(snap)
+    for e in (a, b_eng, c):
+        e.close()

@@ -75,3 +75,17 @@ def test_server_create_fails_loudly_without_gpu():
     with pytest.raises(csm.CsmError) as ei:
         csm.Server()
     assert ei.value.code == -8
+
+
+def test_binary_formats_round_trip(tmp_path):
+    from csm import gen, textio
+    w = gen.make_workload("c1", gen.scaled("c1", 0.05))
+    df, uf = str(tmp_path / "d.bin"), str(tmp_path / "u.bin")
+    textio.write_binary_data(df, w.data)
+    textio.write_binary_updates(uf, w.batches)
+    vl, s, d, l = textio.read_binary_data(df)
+    assert (vl == w.data.vlabels).all() and (s == w.data.src).all() and (d == w.data.dst).all()
+    assert (l == w.data.elabels).all()
+    us, ud, ul, udl = textio.read_binary_updates(uf)
+    assert len(us) == sum(len(b.src) for b in w.batches)
+    assert (us[: len(w.batches[0].src)] == w.batches[0].src).all()
