@@ -104,7 +104,9 @@ def sample_query(adj: Adjacency, vlab: np.ndarray, k: int, kind: str, rng: np.ra
     """Samples a connected k-vertex query from the data graph, so that it has matches.
 
     kind = "tree": a random walk until k distinct vertices are visited; the query is the walk's
-    spanning tree.  kind = "dense": the vertex set grows from a random edge, each step adding the
+    spanning tree.  kind = "sparse": that spanning tree plus 1..k/2 random edges of the data
+    graph among the same vertices (so at least one cycle, average degree below 3; walks whose
+    vertices span no extra edge are retried).  kind = "dense": the vertex set grows from a random edge, each step adding the
     neighbour with the most edges into the set (ties broken at random), and the query is the
     induced subgraph; sets with average degree >= 3 are preferred (the densest after
     `max_tries` otherwise)."""
@@ -126,6 +128,32 @@ def sample_query(adj: Adjacency, vlab: np.ndarray, k: int, kind: str, rng: np.ra
                 steps += 1
             if len(vs) < k:
                 continue
+            return QueryGraph(np.array([vlab[v] for v in vs], dtype=np.uint32),
+                              np.array([e[0] for e in edges], dtype=np.uint32),
+                              np.array([e[1] for e in edges], dtype=np.uint32),
+                              np.array([e[2] for e in edges], dtype=np.uint32))
+        if kind == "sparse":
+            vs, edges, cur, steps = [v0], [], v0, 0
+            while len(vs) < k and steps < 50 * k:
+                nb = adj.nbrs(cur)
+                nxt = int(nb[rng.integers(len(nb))])
+                if nxt not in vs:
+                    vs.append(nxt)
+                    edges.append((vs.index(cur), len(vs) - 1, adj.edge_label(cur, nxt)))
+                cur = nxt
+                steps += 1
+            if len(vs) < k:
+                continue
+            tree = {(min(a, b), max(a, b)) for a, b, _ in edges}
+            ind = _induced(adj, vs, vlab)
+            extra = [(int(a), int(b), int(l)) for a, b, l in zip(ind.src, ind.dst, ind.elabels)
+                     if (int(a), int(b)) not in tree]
+            if not extra:
+                continue
+            order = rng.permutation(len(extra))
+            room = (3 * k - 1) // 2 - (k - 1)
+            take = min(len(extra), room, int(rng.integers(1, max(2, k // 2 + 1))))
+            edges = edges + [extra[i] for i in order[:take]]
             return QueryGraph(np.array([vlab[v] for v in vs], dtype=np.uint32),
                               np.array([e[0] for e in edges], dtype=np.uint32),
                               np.array([e[1] for e in edges], dtype=np.uint32),
@@ -260,11 +288,12 @@ CONFIGS = {
     # LiveJournal-shaped heavy-vertex stress: 4.8M vertices, 43M edges, 20 Zipf(1.2) labels.
     "c3": dict(n=4_800_000, m=43_000_000, gamma=1.9, nvl=20, vzipf=1.2, nel=1, ezipf=None, cap=True,
                n_ins=2_150_000, n_del=2_150_000, batch=1_000_000, queries=[("dense", 8)] * 4),
-    # Batched multi-query: the Amazon-shaped graph, 64 queries of 4..12 vertices.
+    # Batched multi-query: the Amazon-shaped graph, 64 queries of 4..12 vertices, dense and sparse.
     "c4": dict(n=400_000, m=2_400_000, gamma=2.1, nvl=6, vzipf=1.0, nel=1, ezipf=None, cap=True, n_ins=216_000,
                n_del=24_000, batch=65_536, queries="mixed64"),
     # Serving: Netflow-shaped multi-label graph, 32 queries of 4..10 vertices.
-    # Batch sizes are log-uniform in [1k, 256k] (batch_range); `batch` is the largest.
+    # 32 queries of 4..10 vertices, dense and sparse.  Batch sizes are log-uniform in
+    # [1k, 256k] (batch_range); `batch` is the largest.
     "c5": dict(n=3_000_000, m=20_000_000, gamma=2.1, nvl=8, vzipf=None, nel=16, ezipf=1.1, cap=True,
                n_ins=700_000, n_del=300_000, batch=262_144, batch_range=(1_024, 262_144), queries="mixed32"),
 }
@@ -297,7 +326,7 @@ def make_workload(name: str, cfg: Optional[dict] = None, seed: Optional[int] = N
     qspec = cfg["queries"]
     if qspec == "mixed64" or qspec == "mixed32":
         nq, kmax = (64, 12) if qspec == "mixed64" else (32, 10)
-        qspec = [("dense" if i % 2 == 0 else "tree", int(np.random.default_rng(seed + i).integers(4, kmax + 1)))
+        qspec = [("dense" if i % 2 == 0 else "sparse", int(np.random.default_rng(seed + i).integers(4, kmax + 1)))
                  for i in range(nq)]
     if nqueries is not None:
         qspec = qspec[:nqueries]

@@ -840,7 +840,7 @@ csm_status Engine::enqueue_batch(uint64_t n, const uint32_t *src, const uint32_t
 csm_status Engine::enqueue_readback(cudaStream_t s) {
     const uint32_t np = (uint32_t)plans_.size();
     unsigned int *h_err = reinterpret_cast<unsigned int *>(h_counts_ + 2 * np + 3);
-    CSM_CUDA(cudaEventRecord(ev_[1], s));
+    CSM_CUDA(record_event(ev_[1], s));
     CSM_CUDA(cudaMemcpyAsync(h_counts_, d_counts_, 2 * sizeof(unsigned long long) * np, cudaMemcpyDeviceToHost, s));
     CSM_CUDA(cudaMemcpyAsync(h_counts_ + 2 * np, bs_.counters, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                              s));
@@ -863,8 +863,10 @@ csm_status Engine::launch_graph(uint64_t n, bool has_delete, cudaStream_t s) {
         if (graphs_.size() >= 8) clear_graphs();
         const Stats0 before{stats_.kernel_launches, stats_.enum_launches};
         CSM_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+        capturing_ = true;
         const csm_status st = enqueue_batch(n, d_upd_src_, d_upd_dst_, d_upd_lab_, has_delete ? d_upd_del_ : nullptr,
                                             has_delete, false, s);
+        capturing_ = false;
         cudaGraph_t g = nullptr;
         const cudaError_t ce = cudaStreamEndCapture(s, &g);
         if (st != CSM_OK) {
@@ -1040,9 +1042,9 @@ csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
     const int strategy = lc_.strategy;
     const int ph = phase == CSM_PHASE_INS ? 1 : 0;
     phase_ran_[ph] = true;
-    CSM_CUDA(cudaEventRecord(ev_[2 + 2 * ph], s));
+    CSM_CUDA(record_event(ev_[2 + 2 * ph], s));
 
-    launch_ctrl_reset(sc_.ctrl, total_warps, 0, s);
+    launch_ctrl_reset(sc_.ctrl, 0, 0, s);
     launch_seed_tickets(d_plans_, np, d_keys_, m, kl_, sc_.seed_lo, sc_.ticket_prefix, sc_.ctrl, s);
     stats_.kernel_launches += 3;
     const WorkItem *frontier = nullptr;
@@ -1078,7 +1080,7 @@ csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
             X.frontier = frontier;
             X.expand_out = d_frontier_[buf];
             X.expand_cap = frontier_cap_;
-            if (frontier) launch_ctrl_reset(sc_.ctrl, total_warps, nfront, s);
+            if (frontier) launch_ctrl_reset(sc_.ctrl, 0, nfront, s);
             launch_enumerate(X, blocks_, warps_per_block_, occupancy_, s);
             stats_.enum_launches++;
             stats_.kernel_launches++;
@@ -1101,13 +1103,13 @@ csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
     D.donate = (strategy == 0 || strategy == 2) ? 1u : 0u;
     if (frontier) {
         D.frontier = frontier;
-        launch_ctrl_reset(sc_.ctrl, total_warps, nfront, s);
+        launch_ctrl_reset(sc_.ctrl, 0, nfront, s);
         stats_.kernel_launches++;
     }
     launch_enumerate(D, blocks_, warps_per_block_, occupancy_, s);
     stats_.enum_launches++;
     stats_.kernel_launches++;
-    CSM_CUDA(cudaEventRecord(ev_[3 + 2 * ph], s));
+    CSM_CUDA(record_event(ev_[3 + 2 * ph], s));
     // Statistics and error bits are read after the batch's final synchronisation.
     CSM_CUDA(cudaMemcpyAsync(&h_ctrl_[ph], sc_.ctrl, sizeof(EnumControl), cudaMemcpyDeviceToHost, s));
     if (rows) {

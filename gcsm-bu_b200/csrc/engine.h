@@ -190,6 +190,12 @@ class Engine {
         uint64_t kernels, enum_launches;
     };
     std::vector<GraphEntry> graphs_;
+    bool capturing_ = false;
+    // Timing events inside a captured graph must be event-record nodes (external events);
+    // outside a capture they are ordinary records.
+    cudaError_t record_event(cudaEvent_t e, cudaStream_t s) const {
+        return cudaEventRecordWithFlags(e, s, capturing_ ? cudaEventRecordExternal : cudaEventRecordDefault);
+    }
     uint64_t graph_gen_ = 0;  // bumped whenever a buffer a graph refers to is reallocated
     bool graphs_on() const {
         return cfg_.cuda_graphs && !no_alloc_ && lc_.strategy < 2 && cfg_.materialize_rows == 0;

@@ -879,6 +879,11 @@ __global__ void __launch_bounds__(256, MINB) k_enumerate(EnumParams P) {
     unsigned long long scans = 0, probes = 0, tails = 0;
     unsigned int err = 0;
     bool have_source = true;  // seed tickets / frontier not yet exhausted
+    // A warp counts as active from its start: blocks that become resident late (the GPU shared
+    // with other kernels, or more blocks than fit) join the count when they start, so warps
+    // that ran out of work never wait for blocks that have not started.
+    if (lane == 0) atomicAdd(&P.ctrl->active, 1u);
+    __syncwarp();
     while (true) {
         int got = 0;
         if (have_source) {
