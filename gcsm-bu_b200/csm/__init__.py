@@ -393,13 +393,13 @@ class Server:
 
     def wait(self, rid: int, timeout_ms: int = -1):
         """Returns (info, per-query results), or None if the request is still running."""
-        n = self._nres[rid]
+        n = self._nres.get(rid, 0)
         out = (CsmBatchResult * max(1, n))()
         info = CsmRequestInfo()
         rc = self.lib.csm_server_wait(self._h, rid, timeout_ms, ctypes.byref(info), out, n)
         if rc == -4:
             return None
-        del self._nres[rid]
+        self._nres.pop(rid, None)
         self._check(rc)
         return info, list(out)[:n]
 

@@ -61,6 +61,7 @@ struct __align__(16) WarpState {
     uint32_t ts_off[CSM_TAIL_MAXKEYS];
     uint32_t ts_size[CSM_TAIL_MAXKEYS];
     uint32_t ts_base[CSM_TAIL_MAXKEYS];
+    uint32_t ts_cur[CSM_TAIL_MAXKEYS];  // cursor of the shared list over ascending candidates
     uint32_t item_plan;
     uint32_t item_depth;
     uint32_t item_lo;
@@ -141,6 +142,7 @@ __device__ void prep_tail_shared(WarpState &S, const EnumParams &P, const DevPla
             S.ts_off[lane] = ms.x;
             S.ts_size[lane] = ms.y;
             S.ts_base[lane] = left;
+            S.ts_cur[lane] = 0;
         }
     }
     __syncwarp();
@@ -150,7 +152,8 @@ __device__ void prep_tail_shared(WarpState &S, const EnumParams &P, const DevPla
 // lane's candidate at depth d (for d == 1 the prefix is the seed edge (x0, v)).  Only for
 // plans whose masks are single keys (no list intersections).
 __device__ unsigned long long tail_count_lane(const WarpState &S, const EnumParams &P, const DevPlan *pl,
-                                              uint32_t d, uint32_t x0, uint32_t v, unsigned long long &probes) {
+                                              uint32_t d, uint32_t x0, uint32_t v, uint32_t shared_hit,
+                                              unsigned long long &probes) {
     const DevTail *T = &pl->tail;
     const uint32_t nkeys = __ldg(&T->nkeys);
     uint32_t ksize[CSM_TAIL_MAXKEYS];
@@ -162,11 +165,10 @@ __device__ unsigned long long tail_count_lane(const WarpState &S, const EnumPara
         const bool old = __ldg(&T->key_old[k]) != 0;
         uint32_t left;
         if (pd < d && d >= 2) {
-            // Shared list: only this lane's candidate may still sit in it.
-            left = S.ts_base[k];
-            const uint32_t e = find_entry(P.g.pool + S.ts_off[k], S.ts_size[k], v);
-            probes++;
-            if (e != 0xFFFFFFFFu && !(old && (e & 1u))) left--;
+            // Shared list: only this lane's candidate may still sit in it (looked up by the
+            // warp beforehand, bit k of shared_hit).
+            left = S.ts_base[k] - ((shared_hit >> k) & 1u);
+            (void)old;
         } else {
             const uint32_t x = (pd == d) ? v : x0;  // d >= 2: pd == d; d == 1: parent 0 or 1
             const uint2 ms = __ldg(P.g.meta + (size_t)rel * P.g.V + x);
@@ -821,14 +823,51 @@ __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, unsign
             }
             __syncwarp();
         } else if (d + 1 == E && E < n && pl->tail.lane_par) {
-            // Counting level before the tail: every surviving lane sizes its own tail.
+            // Counting level before the tail: every surviving lane sizes its own tail.  Lists
+            // shared by the chunk (parent matched above this level) are searched by the warp
+            // with a cursor, as the probe lists are: the chunk's candidates ascend.
+            uint32_t shared_hit = 0;
+            if (d >= 2) {
+                const DevTail *T = &pl->tail;
+                const uint32_t nkeys = __ldg(&T->nkeys);
+                const uint32_t vm = __ballot_sync(0xffffffffu, idx < S.hi[d]);
+                const uint32_t tgt = __shfl_sync(0xffffffffu, cand, 31 - __clz(vm));
+                const uint32_t key_hi = (tgt + 1) << 1;
+                for (uint32_t k = 0; k < nkeys; k++) {
+                    if (__ldg(&T->key_parent[k]) >= d) continue;
+                    if (!__any_sync(0xffffffffu, ok)) break;
+                    const uint32_t *L = P.g.pool + S.ts_off[k];
+                    const uint32_t size = S.ts_size[k];
+                    const uint32_t c0 = S.ts_cur[k];
+                    const uint32_t win = c0 + lane < size ? __ldg(L + c0 + lane) : 0xFFFFFFFFu;
+                    const uint32_t below = __ballot_sync(0xffffffffu, win < key_hi);
+                    uint32_t e = 0xFFFFFFFFu, hi;
+                    if (below != 0xffffffffu) {
+                        hi = c0 + __popc(below);
+                        const uint32_t pos = shfl_lower_bound(win, cand << 1);
+                        const uint32_t got = __shfl_sync(0xffffffffu, win, pos);
+                        if ((got >> 1) == cand && got != 0xFFFFFFFFu) e = got;
+                    } else {
+                        hi = warp_lower_bound(L, c0 + 32, size, key_hi, lane);
+                        if (ok) e = find_entry(L + c0, hi - c0, cand);
+                    }
+                    __syncwarp();
+                    if (lane == 0) S.ts_cur[k] = hi;
+                    if (ok) {
+                        probes++;
+                        const bool old_k = __ldg(&T->key_old[k]) != 0;
+                        if (e != 0xFFFFFFFFu && !(old_k && (e & 1u))) shared_hit |= 1u << k;
+                    }
+                }
+                __syncwarp();
+            }
             unsigned long long t = 0;
             if (ok) {
                 if (d == 1) {
                     const unsigned long long key = __ldg(P.keys + cand);
-                    t = tail_count_lane(S, P, pl, 1, P.kl.src(key), P.kl.dst(key), probes);
+                    t = tail_count_lane(S, P, pl, 1, P.kl.src(key), P.kl.dst(key), 0, probes);
                 } else {
-                    t = tail_count_lane(S, P, pl, d, 0, cand, probes);
+                    t = tail_count_lane(S, P, pl, d, 0, cand, shared_hit, probes);
                 }
             }
             for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
