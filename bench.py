@@ -309,7 +309,15 @@ def run_ours(args, w, world, rank, local):
     tmax = max_over_ranks(t, world, dev)
     sts = [e.stats() for e in engines]
 
-    # End to end: host (pinned) update arrays through csm_apply_batch, the next steps.
+    # End to end: the same steps again from host (pinned) update arrays through
+    # csm_apply_batch.  Every stream batch only inserts absent edges and deletes present ones,
+    # so applying the inverses of the timed steps in reverse order (untimed) restores the
+    # state the timed region started from.
+    undo = [(qi, inverse(b)) for qi, b in reversed(timed)]
+    for qi, b in undo:
+        apply_dev(qi, b)
+    torch.cuda.synchronize(dev)
+    timed_e2e = timed
     pinned = {}
     for _, b in timed_e2e:
         if id(b) not in pinned:
@@ -364,7 +372,9 @@ def run_ours(args, w, world, rank, local):
         "p50_batch_ms": float(np.percentile(lat, 50)), "p99_batch_ms": float(np.percentile(lat, 99)),
         "matches_per_step": matches / args.steps,
         "e2e": {"value": world * matches_e2e / t_e2e_max, "unit": "matches/s",
-                "h2d_bytes_per_step": h2d // max(1, len(timed_e2e)), "d2h_bytes_per_step": 64},
+                "h2d_bytes_per_step": h2d // max(1, len(timed_e2e)), "d2h_bytes_per_step": 64,
+                "steps": "the timed steps again (state restored by their inverses)",
+                "counts_equal_to_device_run": matches_e2e == matches},
         "gpu_launches": int(sum(st.kernel_launches for st in sts)),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": f"{peak_kind} hbm_gbs",
@@ -461,6 +471,14 @@ def run_batched(args, w, world, rank, local):
     tmax = max_over_ranks(t, world, dev)
     st = eng.stats()
 
+    # The same batches again through the host API, from the state the timed region started
+    # from (restored by applying the inverses of the timed batches in reverse order).
+    for b in [inverse(b) for b in reversed(timed)]:
+        dev_cache[id(b)] = device_arrays(b, dev)
+        apply_dev(eng, b)
+        del dev_cache[id(b)]
+    torch.cuda.synchronize(dev)
+    timed_e2e = timed
     pinned = {}
     for b in timed_e2e:
         if id(b) not in pinned:
@@ -533,7 +551,9 @@ def run_batched(args, w, world, rank, local):
         "speedup_vs_plain": (batched_first / t_first) / (plain_matches / plain_tmax) if plain_matches and t_first else None,
         "counts_identical_to_plain": bool(identical),
         "e2e": {"value": world * matches_e2e / t_e2e_max, "unit": "matches/s",
-                "h2d_bytes_per_step": h2d // max(1, len(timed_e2e)), "d2h_bytes_per_step": 64 * len(w.queries)},
+                "h2d_bytes_per_step": h2d // max(1, len(timed_e2e)), "d2h_bytes_per_step": 64 * len(w.queries),
+                "steps": "the timed batches again (state restored by their inverses)",
+                "counts_equal_to_device_run": matches_e2e == matches},
         "gpu_launches": int(st.kernel_launches),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": f"{peak_kind} hbm_gbs", "kernel": "k_enumerate",

@@ -70,7 +70,7 @@ class CsmConfig(ctypes.Structure):
         ("autotune_batches", ctypes.c_int32),
         ("cuda_graphs", ctypes.c_int32),
         ("replan_drift_pct", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 1),
+        ("semi_bfs_items_per_warp", ctypes.c_int32),
     ]
 
 

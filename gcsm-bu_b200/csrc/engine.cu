@@ -103,15 +103,33 @@ csm_status Engine::init() {
     lc.steal_chunk = cfg_.steal_chunk > 0 ? (uint32_t)cfg_.steal_chunk : 64u;
     lc.warps_per_block = warps_per_block_;
     lc.occupancy = cfg_.occupancy >= 4 && cfg_.occupancy <= 6 ? cfg_.occupancy : 4;
-    lc.frontier_mult = 8;
+    lc.frontier_mult = cfg_.semi_bfs_items_per_warp > 0 ? (uint32_t)cfg_.semi_bfs_items_per_warp : 8u;
     set_launch_config(lc);
     if (cfg_.autotune_batches > 0) {
-        // Candidates: the configured one first, then variations of one knob each.
+        // Candidates: the configured one first, then variations of one knob each: the search
+        // strategy (depth first with stealing, dynamic semi-BFS, BFS while the frontier fits),
+        // the semi-BFS frontier target, steal granularity, warps per block and the
+        // 6-blocks-per-SM kernel variant.
         tune_cands_.push_back(lc);
-        auto add = [&](LaunchConfig c) { tune_cands_.push_back(c); };
-        LaunchConfig c = lc;
-        c.strategy = lc.strategy == 0 ? 2 : 0;
-        add(c);
+        auto add = [&](LaunchConfig c) {
+            for (auto &o : tune_cands_)
+                if (o.strategy == c.strategy && o.steal_chunk == c.steal_chunk && o.warps_per_block == c.warps_per_block &&
+                    o.occupancy == c.occupancy && o.frontier_mult == c.frontier_mult)
+                    return;
+            tune_cands_.push_back(c);
+        };
+        LaunchConfig c;
+        for (int st : {0, 2, 3}) {
+            c = lc;
+            c.strategy = st;
+            add(c);
+        }
+        for (uint32_t fm : {64u, 512u}) {
+            c = lc;
+            c.strategy = 2;
+            c.frontier_mult = fm;
+            add(c);
+        }
         c = lc;
         c.steal_chunk = 256;
         add(c);
@@ -119,13 +137,8 @@ csm_status Engine::init() {
         c.warps_per_block = 4;
         add(c);
         c = lc;
-        c.occupancy = 5;
+        c.occupancy = 6;
         add(c);
-        if (lc.strategy >= 2) {
-            c = lc;
-            c.frontier_mult = 64;
-            add(c);
-        }
         tune_ms_.assign(tune_cands_.size(), 0.0);
         tune_left_ = cfg_.autotune_batches;
         for (size_t i = 0; i < 2 * tune_cands_.size(); i++) CSM_CUDA(cudaEventCreate(&tune_ev_[i]));

@@ -80,7 +80,8 @@ typedef struct csm_config {
     int32_t replan_drift_pct;       /* >0: re-plan the matching orders after a batch that moved a
                                        relation's size by more than this percentage since the last
                                        planning (the reference plans once, before the stream) */
-    int32_t reserved[1];
+    int32_t semi_bfs_items_per_warp; /* dynamic semi-BFS (strategy 2) stops expanding once the
+                                       frontier holds this many items per warp; 0 = 8 */
 } csm_config;
 
 /* Per-query result of one batch. */

@@ -158,10 +158,10 @@ def test_autotune_keeps_counts_and_reports_choice():
     for b in w.batches[:3]:
         eng.apply(b)
     st = eng.stats()
-    assert st.tuned_strategy in (0, 2)
+    assert st.tuned_strategy in (0, 2, 3)
     assert st.tuned_steal_chunk in (64, 256)
     assert st.tuned_warps_per_block in (4, 8)
-    assert st.tuned_occupancy in (4, 5)
+    assert st.tuned_occupancy in (4, 6)
     eng.close()
 
 

@@ -72,7 +72,7 @@ def served(w, groups, batches, slots, budget, per_tenant=False, **cfg):
 
 @pytest.fixture(scope="module")
 def wl():
-    return small_workload("c2", scale=0.004, batch=2500, nqueries=6)
+    return small_workload("c2", scale=0.004, batch=300, nqueries=6)
 
 
 def test_alone_matches_oracle(wl):
