@@ -51,7 +51,8 @@ def parse():
     ap.add_argument("--form", default="plain", choices=["plain", "batched", "served"],
                     help="plain: one engine per standing query, a step is one batch for one query; "
                          "batched: one engine for all standing queries, a step is one batch for all of them")
-    ap.add_argument("--autotune", type=int, default=0, help="batched form: batches the engine tunes its launch on")
+    ap.add_argument("--autotune", type=int, default=3,
+                    help="batched and served forms: batches each engine tunes its launch on (within the warm-up)")
     ap.add_argument("--tenants", type=int, default=4, help="served form: query groups, one graph replica each")
     ap.add_argument("--slots", type=int, default=4, help="served form: concurrent work units")
     ap.add_argument("--rate", type=float, default=50.0, help="served form: Poisson arrival rate (batches/s)")
@@ -594,9 +595,10 @@ def run_served(args, w, world, rank, local):
     stream = torch.cuda.current_stream(dev)
     groups = split_queries(w.queries, max(1, min(args.tenants, len(w.queries))))
     engines = []
+    tune = min(args.autotune, args.warmup)
     for g in groups:
         e = csm.Engine(device=local, algorithm=0, search_strategy=args.strategy, max_batch=w.batch_size,
-                       frontier_bytes=1 << 20)
+                       frontier_bytes=1 << 20, autotune_batches=tune)
         for qi in g:
             e.load_query(w.queries[qi])
         e.load_graph(w.data)
@@ -708,6 +710,7 @@ def run_served(args, w, world, rank, local):
                                f" requests = stream batches of {min(sizes)}..{max(sizes)} updates (stream, then"
                                " its inverse), each for every tenant",
                    "tenants": len(groups), "slots": args.slots, "memory_budget_gb": args.budget_gb,
+                   "autotune_batches": tune,
                    "search_strategy": args.strategy, "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (20M-edge graph replicas, 126 MB L2)"},
         "poisson": {"rate_per_s": args.rate, "requests": len(infos_p),
@@ -717,6 +720,8 @@ def run_served(args, w, world, rank, local):
         "p50_batch_ms": float(np.percentile(lat, 50)), "p99_batch_ms": float(np.percentile(lat, 99)),
         "burst_p50_ms": float(np.percentile(lat_b, 50)), "burst_p99_ms": float(np.percentile(lat_b, 99)),
         "update_edges_per_s": world * sum(len(b.src) for b in burst) / span_b_max,
+        "tuned": [{"strategy": st.tuned_strategy, "steal_chunk": st.tuned_steal_chunk,
+                   "warps_per_block": st.tuned_warps_per_block, "occupancy": st.tuned_occupancy} for st in sts],
         "server": {"units": sst.units, "units_depth_first": sst.units_depth_first, "units_shrunk": sst.units_shrunk,
                    "memory_waits": sst.memory_waits, "peak_frontier_mb": sst.peak_frontier_bytes / 2 ** 20,
                    "peak_inflight": sst.peak_inflight},

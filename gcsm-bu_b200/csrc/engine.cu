@@ -1113,7 +1113,9 @@ csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
     }
     EnumParams D = P;
     D.mode = rows ? CSM_ENUM_MODE_ROWS : CSM_ENUM_MODE_COUNT;
-    D.donate = (strategy == 0 || strategy == 2) ? 1u : 0u;
+    // Work donation in the depth-first launch for every strategy but 1 ("DFS w/o work
+    // stealing"); after a BFS phase (strategy 3) it evens out the frontier items' subtrees.
+    D.donate = strategy == 1 ? 0u : 1u;
     if (frontier) {
         D.frontier = frontier;
         launch_ctrl_reset(sc_.ctrl, 0, nfront, s);
