@@ -103,7 +103,7 @@ csm_status Engine::init() {
     lc.steal_chunk = cfg_.steal_chunk > 0 ? (uint32_t)cfg_.steal_chunk : 64u;
     lc.warps_per_block = warps_per_block_;
     lc.occupancy = cfg_.occupancy >= 4 && cfg_.occupancy <= 6 ? cfg_.occupancy : 4;
-    lc.frontier_mult = cfg_.semi_bfs_items_per_warp > 0 ? (uint32_t)cfg_.semi_bfs_items_per_warp : 8u;
+    lc.frontier_mult = cfg_.semi_bfs_items_per_warp > 0 ? (uint32_t)cfg_.semi_bfs_items_per_warp : 512u;
     set_launch_config(lc);
     if (cfg_.autotune_batches > 0) {
         // Candidates: the configured one first, then variations of one knob each: the search
@@ -124,7 +124,7 @@ csm_status Engine::init() {
             c.strategy = st;
             add(c);
         }
-        for (uint32_t fm : {64u, 512u}) {
+        for (uint32_t fm : {8u, 64u, 512u}) {
             c = lc;
             c.strategy = 2;
             c.frontier_mult = fm;
@@ -1238,6 +1238,11 @@ void Engine::reset_stats() {
     std::memset(&stats_, 0, sizeof(stats_));
     stats_.pool_used = used;
     stats_.pool_capacity = cap;
+    // The launch configuration in use is state, not a counter.
+    stats_.tuned_strategy = (uint64_t)lc_.strategy;
+    stats_.tuned_steal_chunk = lc_.steal_chunk;
+    stats_.tuned_warps_per_block = (uint64_t)lc_.warps_per_block;
+    stats_.tuned_occupancy = (uint64_t)lc_.occupancy;
 }
 
 csm_status Engine::memory(uint64_t *free_b, uint64_t *total_b) const {

@@ -94,6 +94,8 @@ class Engine {
     uint64_t enum_warps() const { return (uint64_t)blocks_ * (uint64_t)warps_per_block_; }
     // Search strategy of the launch configuration in use (0..3).
     int strategy() const { return lc_.strategy; }
+    // Frontier items at which the dynamic semi-BFS stops expanding.
+    uint64_t semi_bfs_target_items() const { return (uint64_t)lc_.frontier_mult * enum_warps(); }
     uint64_t batch_capacity() const { return batch_cap_; }
     int device() const { return device_; }
     cudaStream_t stream() const { return stream_; }

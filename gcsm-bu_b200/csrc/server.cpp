@@ -277,12 +277,11 @@ class Server {
 
   private:
     // Frontier bytes a unit asks for: two buffers of twice the items the tenant's semi-BFS
-    // wrote per update recently, scaled to this batch, and at least the item count at which
-    // the dynamic semi-BFS switches to depth first (64 items per warp).  Depth-first tenants
-    // need none.
+    // wrote per update recently, scaled to this batch, and at least twice the item count at
+    // which the dynamic semi-BFS switches to depth first.  Depth-first tenants need none.
     uint64_t estimate(const Tenant &t, uint64_t n) const {
         if (t.eng->strategy() < 2) return 0;
-        const double floor_items = 64.0 * (double)t.eng->enum_warps();
+        const double floor_items = 2.0 * (double)t.eng->semi_bfs_target_items();
         const double items = std::max(floor_items, 2.0 * t.rows_per_update * (double)n);
         const double bytes = 2.0 * items * (double)sizeof(WorkItem);
         return (uint64_t)std::min(bytes, (double)arena_.size());

@@ -81,7 +81,7 @@ typedef struct csm_config {
                                        relation's size by more than this percentage since the last
                                        planning (the reference plans once, before the stream) */
     int32_t semi_bfs_items_per_warp; /* dynamic semi-BFS (strategy 2) stops expanding once the
-                                       frontier holds this many items per warp; 0 = 8 */
+                                       frontier holds this many items per warp; 0 = 512 */
 } csm_config;
 
 /* Per-query result of one batch. */
