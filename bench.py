@@ -53,7 +53,7 @@ def parse():
                          "batched: one engine for all standing queries, a step is one batch for all of them")
     ap.add_argument("--autotune", type=int, default=3,
                     help="batched and served forms: batches each engine tunes its launch on (within the warm-up)")
-    ap.add_argument("--tenants", type=int, default=4, help="served form: query groups, one graph replica each")
+    ap.add_argument("--tenants", type=int, default=1, help="served form: query groups, one graph replica each")
     ap.add_argument("--slots", type=int, default=4, help="served form: concurrent work units")
     ap.add_argument("--rate", type=float, default=50.0, help="served form: Poisson arrival rate (batches/s)")
     ap.add_argument("--budget-gb", type=float, default=80.0, help="served form: frontier memory budget")
@@ -500,7 +500,7 @@ def run_batched(args, w, world, rank, local):
     # The plain path on the same batches: one engine per query, each batch applied to each.
     nplain = args.steps if args.plain_steps is None else min(args.plain_steps, args.steps)
     plain_t, plain_matches, identical = 0.0, 0, True
-    for qi, q in enumerate(w.queries):
+    for qi, q in enumerate(w.queries if nplain else []):
         e = csm.Engine(device=local, algorithm=0, search_strategy=args.strategy, max_batch=w.batch_size)
         e.load_query(q)
         e.load_graph(w.data)
@@ -667,7 +667,7 @@ def run_served(args, w, world, rank, local):
     nplain = len(burst) if args.plain_steps is None else min(args.plain_steps, len(burst))
     plain_t, plain_matches, identical = 0.0, 0, True
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    for qi, q in enumerate(w.queries):
+    for qi, q in enumerate(w.queries if nplain else []):
         e = csm.Engine(device=local, algorithm=0, search_strategy=args.strategy, max_batch=w.batch_size)
         e.load_query(q)
         e.load_graph(w.data)
@@ -692,7 +692,8 @@ def run_served(args, w, world, rank, local):
     if rank != 0:
         return
     served_first = sum(p + n for row in rows_b[:nplain] for p, n in row)
-    served_first_t = (max(i.done_ns for i in infos_b[:nplain]) - min(i.arrival_ns for i in infos_b[:nplain])) / 1e9
+    served_first_t = (max(i.done_ns for i in infos_b[:nplain]) - min(i.arrival_ns for i in infos_b[:nplain])) / 1e9 \
+        if nplain else 0.0
     peak, peak_kind = measured_peaks()
     enum_s = sum(st.enum_ns for st in sts) / 1e9
     launches = max(1, sum(st.enum_launches for st in sts))

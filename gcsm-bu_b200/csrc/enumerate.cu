@@ -153,7 +153,7 @@ __device__ void prep_tail_shared(WarpState &S, const EnumParams &P, const DevPla
 // plans whose masks are single keys (no list intersections).
 __device__ unsigned long long tail_count_lane(const WarpState &S, const EnumParams &P, const DevPlan *pl,
                                               uint32_t d, uint32_t x0, uint32_t v, uint32_t shared_hit,
-                                              unsigned long long &probes) {
+                                              uint32_t &probes) {
     const DevTail *T = &pl->tail;
     const uint32_t nkeys = __ldg(&T->nkeys);
     uint32_t ksize[CSM_TAIL_MAXKEYS];
@@ -248,7 +248,7 @@ __device__ void enter_level(WarpState &S, const EnumParams &P, const DevPlan *pl
 
 // Number of injective assignments of the tail leaves for the full prefix f[0..E-1].
 __device__ unsigned long long tail_count(WarpState &S, const EnumParams &P, const DevPlan *pl,
-                                         unsigned long long &probes) {
+                                         uint32_t &probes) {
     const uint32_t lane = lane_id();
     const DevTail *T = &pl->tail;
     const uint32_t nkeys = __ldg(&T->nkeys);
@@ -528,7 +528,7 @@ __device__ void write_row(const EnumParams &P, const DevPlan *pl, const WarpStat
 // bitmap, membership in the other backward lists by binary search).  Returns false (nothing
 // counted) when the lists are long enough for the per-sibling scan to fill the warp.
 __device__ bool count_last_packed(WarpState &S, const EnumParams &P, const DevPlan *pl, uint32_t d,
-                                  unsigned long long &cnt, unsigned long long &scans, unsigned long long &probes) {
+                                  unsigned long long &cnt, uint32_t &scans, uint32_t &probes) {
     const uint32_t lane = lane_id();
     const uint32_t L = d + 1;
     const DevLevel *lv = &pl->lv[L];
@@ -625,8 +625,8 @@ __device__ bool count_last_packed(WarpState &S, const EnumParams &P, const DevPl
 }
 
 // Runs one work item to completion.  Returns the number of matches counted.
-__device__ unsigned long long run_item(WarpState &S, const EnumParams &P, unsigned long long &scans,
-                                       unsigned long long &probes, unsigned long long &tails, unsigned int &err) {
+__device__ unsigned long long run_item(WarpState &S, const EnumParams &P, uint32_t &scans,
+                                       uint32_t &probes, uint32_t &tails, unsigned int &err) {
     const uint32_t lane = lane_id();
     const DevPlan *pl = P.plans + S.item_plan;
     const uint32_t n = pl->n;
@@ -915,7 +915,9 @@ __global__ void __launch_bounds__(256, MINB) k_enumerate(EnumParams P) {
     WarpState &S = reinterpret_cast<WarpState *>(smem)[threadIdx.x >> 5];
     const uint32_t lane = lane_id();
     if (P.abort_flag != nullptr && *(volatile const unsigned int *)P.abort_flag) return;
-    unsigned long long scans = 0, probes = 0, tails = 0;
+    // Per-lane work counters (statistics only), 32-bit to keep registers for the search; a
+    // lane flushes them to the launch totals before they could wrap.
+    uint32_t scans = 0, probes = 0, tails = 0;
     unsigned int err = 0;
     bool have_source = true;  // seed tickets / frontier not yet exhausted
     // A warp counts as active from its start: blocks that become resident late (the GPU shared
@@ -965,16 +967,23 @@ __global__ void __launch_bounds__(256, MINB) k_enumerate(EnumParams P) {
         }
         const unsigned long long c = run_item(S, P, scans, probes, tails, err);
         if (lane == 0 && c) atomicAdd(P.counts + S.item_plan, c);
+        if ((scans | probes | tails) >= (1u << 30)) {
+            atomicAdd(&P.ctrl->scan_entries, (unsigned long long)scans);
+            atomicAdd(&P.ctrl->probes, (unsigned long long)probes);
+            atomicAdd(&P.ctrl->tail_lists, (unsigned long long)tails);
+            scans = probes = tails = 0;
+        }
         __syncwarp();
     }
+    unsigned long long scans64 = scans, probes64 = probes;
     for (int o = 16; o > 0; o >>= 1) {
-        scans += __shfl_xor_sync(0xffffffffu, scans, o);
-        probes += __shfl_xor_sync(0xffffffffu, probes, o);
+        scans64 += __shfl_xor_sync(0xffffffffu, scans64, o);
+        probes64 += __shfl_xor_sync(0xffffffffu, probes64, o);
     }
     if (lane == 0) {
-        if (scans) atomicAdd(&P.ctrl->scan_entries, scans);
-        if (probes) atomicAdd(&P.ctrl->probes, probes);
-        if (tails) atomicAdd(&P.ctrl->tail_lists, tails);
+        if (scans64) atomicAdd(&P.ctrl->scan_entries, scans64);
+        if (probes64) atomicAdd(&P.ctrl->probes, probes64);
+        if (tails) atomicAdd(&P.ctrl->tail_lists, (unsigned long long)tails);
         if (err) atomicOr(&P.ctrl->error, err);
     }
 }
