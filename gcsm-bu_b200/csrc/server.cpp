@@ -22,6 +22,7 @@
 
 #include "../../include/csm_server.h"
 #include "engine_handle.h"
+#include "frontier_arena.h"
 
 namespace csm {
 namespace {
@@ -32,68 +33,39 @@ uint64_t now_ns() {
         .count();
 }
 
-constexpr uint64_t kGranule = 256;
 constexpr uint32_t kSlotQueueItems = 1u << 21;
 constexpr uint32_t kSlotMaxPlans = 4096;
 
-// First-fit sub-allocator over one device allocation; free ranges are kept by offset and
-// merged with their neighbours when released.
+// The device range behind the frontier arena (bookkeeping in RangeAllocator).
 class FrontierArena {
   public:
     cudaError_t init(uint64_t bytes) {
-        size_ = bytes / kGranule * kGranule;
-        if (size_ == 0) return cudaSuccess;
-        cudaError_t e = cudaMalloc(&base_, size_);
-        if (e != cudaSuccess) return e;
-        free_[0] = size_;
-        return cudaSuccess;
+        ra_.reset(bytes);
+        if (!ra_.size()) return cudaSuccess;
+        cudaError_t e = cudaMalloc(&base_, ra_.size());
+        if (e != cudaSuccess) ra_.reset(0);
+        return e;
     }
     void release() {
         if (base_) cudaFree(base_);
         base_ = nullptr;
-        free_.clear();
+        ra_.reset(0);
     }
-    // Grants min(want, largest free range) bytes if that is at least `least`; else 0.
     uint64_t take(uint64_t want, uint64_t least, char **ptr) {
-        want = (want + kGranule - 1) / kGranule * kGranule;
-        auto best = free_.end();
-        for (auto it = free_.begin(); it != free_.end(); ++it)
-            if (best == free_.end() || it->second > best->second) best = it;
-        if (best == free_.end()) return 0;
-        const uint64_t got = std::min(want, best->second);
-        if (got == 0 || got < least) return 0;
-        const uint64_t off = best->first, len = best->second;
-        free_.erase(best);
-        if (len > got) free_[off + got] = len - got;
-        used_ += got;
-        *ptr = base_ + off;
+        uint64_t off = 0;
+        const uint64_t got = ra_.take(want, least, &off);
+        if (got) *ptr = base_ + off;
         return got;
     }
     void give(char *ptr, uint64_t bytes) {
-        if (!bytes) return;
-        uint64_t off = (uint64_t)(ptr - base_);
-        used_ -= bytes;
-        auto next = free_.lower_bound(off);
-        if (next != free_.end() && next->first == off + bytes) {
-            bytes += next->second;
-            next = free_.erase(next);
-        }
-        if (next != free_.begin()) {
-            auto prev = std::prev(next);
-            if (prev->first + prev->second == off) {
-                prev->second += bytes;
-                return;
-            }
-        }
-        free_[off] = bytes;
+        if (bytes) ra_.give((uint64_t)(ptr - base_), bytes);
     }
-    uint64_t used() const { return used_; }
-    uint64_t size() const { return size_; }
+    uint64_t used() const { return ra_.used(); }
+    uint64_t size() const { return ra_.size(); }
 
   private:
     char *base_ = nullptr;
-    uint64_t size_ = 0, used_ = 0;
-    std::map<uint64_t, uint64_t> free_;
+    RangeAllocator ra_;
 };
 
 struct Request {
