@@ -158,7 +158,7 @@ Engine::~Engine() {
                    g_.vlab, d_plans_, d_terms_, d_upd_src_, d_upd_dst_, d_upd_lab_, d_upd_del_, d_keys_raw_, d_keys_,
                    d_sort_temp_, bs_.eff, bs_.heads, bs_.nheads, bs_.seg_nins, bs_.seg_ndel, bs_.seg_end, bs_.scr_y,
                    bs_.scr_lb, bs_.counters, bs_.error, d_ctrl_, d_queue_, d_ready_, d_seed_lo_, d_ticket_prefix_,
-                   d_counts_, d_frontier_[0], d_frontier_[1], d_rows_, d_misc_, d_rel_delta_};
+                   d_counts_, d_frontier_[0], d_frontier_[1], d_rows_, d_misc_, d_rel_delta_, d_touched_};
     for (void *p : dev)
         if (p) cudaFree(p);
     if (h_pin_) cudaFreeHost(h_pin_);
@@ -295,6 +295,8 @@ csm_status Engine::prepare_tables(uint32_t nv, const uint32_t *vlabel, const uin
     CSM_CUDA(dalloc(&g_.meta, nmeta));
     CSM_CUDA(dalloc(&g_.cap, nmeta));
     CSM_CUDA(dalloc(&g_.pool_top, 1));
+    CSM_CUDA(dalloc(&d_touched_, words_));
+    CSM_CUDA(cudaMemset(d_touched_, 0, sizeof(uint32_t) * words_));
     return CSM_OK;
 }
 
@@ -806,7 +808,8 @@ csm_status Engine::enqueue_batch(uint64_t n, const uint32_t *src, const uint32_t
         size_t tb = sort_temp_bytes_;
         CSM_CUDA(store_sort_keys(d_sort_temp_, tb, d_keys_raw_, d_keys_, m, kl_, s));
         store_classify(m, d_keys_, kl_, g_, bs_, s);
-        stats_.kernel_launches += 3;
+        store_touched(m, d_keys_, kl_, d_touched_, words_, s);
+        stats_.kernel_launches += 4;
         if (d_rel_delta_) {
             CSM_CUDA(cudaMemsetAsync(d_rel_delta_, 0, sizeof(long long) * g_.R, s));
             store_rel_delta(m, d_keys_, kl_, bs_, d_rel_delta_, s);
@@ -1049,6 +1052,7 @@ csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
     P.idle_limit = 1u << 24;
     P.ready_limit = 1u << 22;
     P.abort_flag = phase == CSM_PHASE_INS ? bs_.error : nullptr;
+    P.touched = d_touched_;
     P.rows = d_rows_;
     P.row_cap = row_cap_;
     const bool rows = cfg_.materialize_rows > 0;

@@ -217,6 +217,7 @@ class Engine {
     csm_status maybe_replan();
     size_t terms_cap_ = 0;
     long long *d_rel_delta_ = nullptr;      // [R] net entry change of the current batch
+    uint32_t *d_touched_ = nullptr;         // [words_] list owners among the batch keys
     long long *h_rel_delta_ = nullptr;      // pinned copy
     std::vector<long long> rel_size_, rel_size_planned_;
     csm_status launch_graph(uint64_t n, bool has_delete, cudaStream_t s);

@@ -114,6 +114,8 @@ __device__ __forceinline__ uint32_t shfl_lower_bound(uint32_t win, uint32_t key2
 
 // Flagged entries of list (rel, x) in this phase (batch edges of that list), 0 if none.
 __device__ __forceinline__ uint32_t flagged_in_list(const EnumParams &P, uint32_t rel, uint32_t x) {
+    // Lists of vertices no batch key starts from hold no batch entry: skip the key search.
+    if (P.touched != nullptr && !((__ldg(P.touched + (x >> 5)) >> (x & 31)) & 1u)) return 0u;
     const unsigned long long lk = P.kl.list_key(rel, x);
     const uint32_t h = find_list_head(P.keys, P.m, P.kl, lk);
     return (h < P.m && P.kl.list_of(__ldg(P.keys + h)) == lk) ? __ldg(P.seg_flagged + h) : 0u;

@@ -107,6 +107,7 @@ struct EnumParams {
     uint32_t idle_limit;             // polls of an idle warp waiting for donated work
     uint32_t ready_limit;            // polls of a claimed slot whose item is being written
     const unsigned int *abort_flag;  // nonzero: the batch update failed, skip enumeration
+    const uint32_t *touched;         // bit per vertex: some batch key has it as list owner
 };
 
 #define CSM_ROW_WORDS (1 + CSM_MAXQV)

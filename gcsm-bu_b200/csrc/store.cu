@@ -422,6 +422,16 @@ __global__ void k_rel_delta(uint32_t m, const unsigned long long *keys, KeyLayou
         atomicAdd(reinterpret_cast<unsigned long long *>(delta + rel), (unsigned long long)(long long)sum);  // two's complement
 }
 
+// Bit per vertex that owns a list some batch key belongs to (the key's source).  Keys are
+// sorted, so neighbouring lanes mostly share a word; one lane per distinct source sets it.
+__global__ void k_touched(uint32_t m, const unsigned long long *keys, KeyLayout kl, uint32_t *bits) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= m) return;
+    const uint32_t x = kl.src(keys[i]);
+    if (i > 0 && kl.src(keys[i - 1]) == x) return;
+    atomicOr(bits + (x >> 5), 1u << (x & 31));
+}
+
 // Entry count of every relation (sum of its list sizes).  The loop is warp-uniform so that all
 // lanes take part in the grouping shuffles.
 __global__ void k_rel_sizes(uint32_t V, uint32_t R, const uint2 *meta, unsigned long long *out) {
@@ -501,6 +511,12 @@ void store_nlf_all(DeviceGraph &g, const NlfTables &nt, cudaStream_t s) {
 void store_rel_delta(uint32_t m, const unsigned long long *keys, KeyLayout kl, const BatchScratch &b, long long *delta,
                      cudaStream_t s) {
     if (m) k_rel_delta<<<(m + 255) / 256, 256, 0, s>>>(m, keys, kl, b.eff, delta);
+}
+
+void store_touched(uint32_t m, const unsigned long long *keys, KeyLayout kl, uint32_t *bits, uint32_t words,
+                   cudaStream_t s) {
+    cudaMemsetAsync(bits, 0, sizeof(uint32_t) * words, s);
+    if (m) k_touched<<<(m + 255) / 256, 256, 0, s>>>(m, keys, kl, bits);
 }
 
 void store_rel_sizes(const DeviceGraph &g, unsigned long long *out, cudaStream_t s) {

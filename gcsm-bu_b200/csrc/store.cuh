@@ -79,6 +79,9 @@ void store_nlf_all(DeviceGraph &g, const NlfTables &nt, cudaStream_t s);
 // Per-relation net entry change of a classified batch (delta[R], accumulated).
 void store_rel_delta(uint32_t m, const unsigned long long *keys, KeyLayout kl, const BatchScratch &b, long long *delta,
                      cudaStream_t s);
+// Bit per vertex owning a list that a batch key belongs to (bits[words], cleared first).
+void store_touched(uint32_t m, const unsigned long long *keys, KeyLayout kl, uint32_t *bits, uint32_t words,
+                   cudaStream_t s);
 // Per-relation entry counts (out[R], accumulated).
 void store_rel_sizes(const DeviceGraph &g, unsigned long long *out, cudaStream_t s);
 void store_edge_stats(DeviceGraph &g, uint32_t rel, const uint32_t *bits_u, const uint32_t *bits_uu,
