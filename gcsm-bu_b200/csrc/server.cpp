@@ -201,7 +201,7 @@ class Server {
         if (info) *info = r->info;
         if (res) std::memcpy(res, r->results.data(), sizeof(csm_batch_result) * std::min<size_t>(cap, r->results.size()));
         const csm_status st = r->info.status;
-        if (st != CSM_OK) err_ = r_err_[id];
+        if (st != CSM_OK) fail(st, r_err_[id]);
         r_err_.erase(id);
         reqs_.erase(it);
         return st;
@@ -237,8 +237,13 @@ class Server {
         started_ = false;
     }
 
-    const std::string &error() const { return err_; }
+    // The last error message (callers may ask from any thread).
+    std::string error() const {
+        std::lock_guard<std::mutex> g(err_mu_);
+        return err_;
+    }
     csm_status fail(csm_status code, const std::string &msg) {
+        std::lock_guard<std::mutex> g(err_mu_);
         err_ = msg;
         return code;
     }
@@ -405,6 +410,7 @@ class Server {
     uint64_t next_id_ = 0;
     uint32_t inflight_ = 0;
     bool stopping_ = false, started_ = false, mem_wait_counted_ = false;
+    mutable std::mutex err_mu_;
     std::string err_;
 };
 
@@ -487,7 +493,7 @@ csm_status csm_server_destroy(csm_server *srv) {
 
 csm_status csm_server_last_error(const csm_server *srv, char *buf, size_t n) {
     if (!buf || !n) return CSM_ERR_INVALID_ARG;
-    const std::string &s = srv ? srv->impl.error() : g_server_create_error;
+    const std::string s = srv ? srv->impl.error() : g_server_create_error;
     const size_t k = std::min(n - 1, s.size());
     std::memcpy(buf, s.data(), k);
     buf[k] = 0;
