@@ -89,3 +89,21 @@ def test_binary_formats_round_trip(tmp_path):
     us, ud, ul, udl = textio.read_binary_updates(uf)
     assert len(us) == sum(len(b.src) for b in w.batches)
     assert (us[: len(w.batches[0].src)] == w.batches[0].src).all()
+
+
+def test_csmg_fails_loudly_without_gpu(tmp_path):
+    ensure_built()
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from csm import gen, textio
+    w = gen.make_workload("c1", gen.scaled("c1", 0.05))
+    qf, df, uf = (str(tmp_path / x) for x in ("q.graph", "d.graph", "u.graph"))
+    textio.write_query(qf, w.queries[0])
+    textio.write_data(df, w.data)
+    textio.write_updates(uf, w.batches)
+    p = subprocess.run([csm.CSMG_PATH, "--query", qf, "--data", df, "--update", uf, "--batch_size", "100"],
+                       capture_output=True, text=True, timeout=60)
+    assert p.returncode != 0
+    assert "Read Graphs from Files" in p.stdout  # parsing ran, then the engine refused
+    assert "no CUDA device" in p.stdout + p.stderr
