@@ -63,6 +63,10 @@ struct DevTail {
     uint8_t key_parent[CSM_TAIL_MAXKEYS];
     uint8_t key_old[CSM_TAIL_MAXKEYS];
     uint16_t key_rel[CSM_TAIL_MAXKEYS];
+    // Per key, bit j set when the query vertex at depth j has the key's leaf label: only the
+    // data vertices matched at those depths can sit in the key's list (labels partition the
+    // relations), so injectivity exclusions search for those alone.
+    uint16_t key_excl[CSM_TAIL_MAXKEYS];
     uint8_t nmasks;                             // key subsets whose intersection size is used
     uint8_t nclasses;
     uint8_t lane_par;                           // every mask is one key: count 32 prefixes per warp step

@@ -136,8 +136,9 @@ __device__ void prep_tail_shared(WarpState &S, const EnumParams &P, const DevPla
             const uint32_t x = S.f[pd];
             const uint2 ms = __ldg(P.g.meta + (size_t)rel * P.g.V + x);
             uint32_t left = ms.y - (old ? flagged_in_list(P, rel, x) : 0u);
+            const uint32_t excl = __ldg(&T->key_excl[lane]);
             for (uint32_t j = 0; j < d; j++) {
-                if (j == pd) continue;
+                if (j == pd || !((excl >> j) & 1u)) continue;
                 const uint32_t e = find_entry(P.g.pool + ms.x, ms.y, S.f[j]);
                 if (e != 0xFFFFFFFFu && !(old && (e & 1u))) left--;
             }
@@ -175,8 +176,9 @@ __device__ unsigned long long tail_count_lane(const WarpState &S, const EnumPara
             const uint32_t x = (pd == d) ? v : x0;  // d >= 2: pd == d; d == 1: parent 0 or 1
             const uint2 ms = __ldg(P.g.meta + (size_t)rel * P.g.V + x);
             left = ms.y - (old ? flagged_in_list(P, rel, x) : 0u);
+            const uint32_t excl = __ldg(&T->key_excl[k]);
             for (uint32_t j = 0; j <= d; j++) {
-                if (j == pd) continue;
+                if (j == pd || !((excl >> j) & 1u)) continue;
                 const uint32_t z = (j == d) ? v : (d == 1 ? x0 : S.f[j]);
                 const uint32_t e = find_entry(P.g.pool + ms.x, ms.y, z);
                 probes++;
@@ -261,20 +263,15 @@ __device__ unsigned long long tail_count(WarpState &S, const EnumParams &P, cons
         const uint2 ms = __ldg(P.g.meta + (size_t)rel * P.g.V + x);
         S.t_off[lane] = ms.x;
         S.t_size[lane] = ms.y;
-        uint32_t fc = 0;
-        if (__ldg(&T->key_old[lane])) {
-            // Flagged entries of this list = batch edges of (rel, x) in this phase.
-            const unsigned long long lk = P.kl.list_key(rel, x);
-            const uint32_t h = find_list_head(P.keys, P.m, P.kl, lk);
-            if (h < P.m && P.kl.list_of(__ldg(P.keys + h)) == lk) fc = __ldg(P.seg_flagged + h);
-        }
-        S.t_flag[lane] = fc;
+        // Flagged entries of this list = batch edges of (rel, x) in this phase.
+        S.t_flag[lane] = __ldg(&T->key_old[lane]) ? flagged_in_list(P, rel, x) : 0u;
         S.t_excl[lane] = 0;
     }
     __syncwarp();
     // Prefix vertices that sit in a tail list are not available to the leaves.
     for (uint32_t pi = lane; pi < nkeys * E; pi += 32) {
         const uint32_t k = pi / E;
+        if (!((__ldg(&T->key_excl[k]) >> (pi % E)) & 1u)) continue;  // other labels are never in the list
         const uint32_t z = S.f[pi % E];
         const uint32_t e = find_entry(P.g.pool + S.t_off[k], S.t_size[k], z);
         if (e != 0xFFFFFFFFu && !(__ldg(&T->key_old[k]) && (e & 1u))) atomicAdd(&S.t_excl[k], 1u);
@@ -837,6 +834,7 @@ __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, uint32
                 const uint32_t key_hi = (tgt + 1) << 1;
                 for (uint32_t k = 0; k < nkeys; k++) {
                     if (__ldg(&T->key_parent[k]) >= d) continue;
+                    if (!((__ldg(&T->key_excl[k]) >> d) & 1u)) continue;  // candidates never in this list
                     if (!__any_sync(0xffffffffu, ok)) break;
                     const uint32_t *L = P.g.pool + S.ts_off[k];
                     const uint32_t size = S.ts_size[k];

@@ -348,6 +348,14 @@ bool build_tail(const Query &q, const HostPlan &hp, int qe, const RelOf &rel_of,
         tail.key_parent[k] = (uint8_t)std::get<0>(keys[k]);
         tail.key_rel[k] = (uint16_t)std::get<1>(keys[k]);
         tail.key_old[k] = (uint8_t)std::get<2>(keys[k]);
+        // A key's relation fixes its leaves' label.
+        uint32_t leaf_label = 0;
+        for (auto &l : leaves)
+            if (l.key == (int)k) leaf_label = l.label;
+        uint16_t excl = 0;
+        for (int d = 0; d < n; d++)
+            if (q.vlabel[hp.order[d]] == leaf_label) excl |= (uint16_t)(1u << d);
+        tail.key_excl[k] = excl;
     }
     std::map<uint32_t, std::vector<int>> classes;  // label -> leaf key ids
     for (auto &l : leaves) classes[l.label].push_back(l.key);

@@ -137,6 +137,10 @@ int main() {
                     for (int k = 0; k < T.nkeys; k++)
                         if (T.key_parent[k] == p && T.key_rel[k] == rel && T.key_old[k] == old) key = k;
                     if (key < 0) return fail("leaf without a tail key", qn, (int)pi);
+                    for (uint32_t j = 0; j < n; j++) {
+                        const bool same = q.vlabel[hp.order[j]] == q.vlabel[u];
+                        if (same != (((T.key_excl[key] >> j) & 1u) != 0)) return fail("exclusion depths", qn, (int)pi);
+                    }
                     leaf_key.push_back(key);
                     leaf_label.push_back(q.vlabel[u]);
                 }
