@@ -107,3 +107,58 @@ def test_rows_sorted_unique_and_counted():
     assert as_tuples == sorted(as_tuples) and len(set(as_tuples)) == len(as_tuples)
     for row in rows:
         assert len(set(row)) == len(row)  # injective
+
+
+def brute_embeddings(q, vlab, edges):
+    """All embeddings of query q (vertex-id order rows) in a small labelled graph given as a
+    set of (min, max, label) edges (one vertex pair may carry edges of several labels, each its
+    own edge, as in the label-partitioned relations), by exhaustive search over injective maps."""
+    import itertools
+    nv = len(q.vlabels)
+    qe = list(zip(q.src.tolist(), q.dst.tolist(), q.elabels.tolist()))
+    out = set()
+    cands = [[v for v in range(len(vlab)) if vlab[v] == q.vlabels[u]] for u in range(nv)]
+    for f in itertools.product(*cands):
+        if len(set(f)) != nv:
+            continue
+        if all((min(f[a], f[b]), max(f[a], f[b]), l) in edges for a, b, l in qe):
+            out.add(tuple(int(x) for x in f))
+    return out
+
+
+@pytest.mark.parametrize("seed", range(24))
+def test_positive_and_negative_rows_against_brute_force(seed):
+    # Independent of any decomposition rule: the positive rows of a batch are exactly the
+    # embeddings of the graph after it that were not embeddings before, the negative rows those
+    # that disappeared; with repeated updates, both orientations and insert+delete of one edge.
+    rng = np.random.default_rng(100 + seed)
+    n = 9
+    vl, s, d, el = random_graph(n, 16, 2, rng, nel=2)
+    data = DataGraph(vl, s, d, el)
+    edges = {(min(int(a), int(b)), max(int(a), int(b)), int(l)) for a, b, l in zip(s, d, el)}
+    adj = gen.Adjacency(n, s, d, el)
+    kind = ["tree", "dense", "sparse"][seed % 3]
+    q = gen.sample_query(adj, vl, 3 + seed % 2, kind, rng)
+    o = Oracle(q, data)
+    for _ in range(3):
+        nb = 8
+        x = rng.integers(0, n, nb).astype(np.uint32)
+        y = rng.integers(0, n, nb).astype(np.uint32)
+        lab = rng.integers(0, 2, nb).astype(np.uint32)
+        dl = (rng.random(nb) < 0.4).astype(np.uint8)
+        if seed % 2:  # repeat one update in the other orientation
+            x[-1], y[-1], lab[-1], dl[-1] = y[0], x[0], lab[0], dl[0]
+        before = brute_embeddings(q, vl, edges)
+        # Set semantics of a batch: deletions of present edges, then insertions of absent ones
+        # (an edge both inserted and deleted in one batch ends present); self-loops are ignored.
+        dels = {(min(int(a), int(b)), max(int(a), int(b)), int(l)) for a, b, l, z in zip(x, y, lab, dl)
+                if z and a != b}
+        ins = {(min(int(a), int(b)), max(int(a), int(b)), int(l)) for a, b, l, z in zip(x, y, lab, dl)
+               if not z and a != b}
+        edges = (edges - dels) | ins
+        after = brute_embeddings(q, vl, edges)
+        r = o.apply(Batch(x, y, lab, dl), rows=True)
+        pos_rows = {tuple(int(v) for v in row) for row in o.rows(1)}
+        neg_rows = {tuple(int(v) for v in row) for row in o.rows(-1)}
+        assert pos_rows == after - before and r["pos"] == len(after - before)
+        assert neg_rows == before - after and r["neg"] == len(before - after)
