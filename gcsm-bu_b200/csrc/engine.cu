@@ -653,6 +653,14 @@ csm_status Engine::load_snapshot(const char *path) {
     for (size_t i = 0; i < nmeta; i++)
         if ((uint64_t)meta[i].x + cap[i] > h.used || meta[i].y > cap[i])
             return fail(CSM_ERR_INVALID_ARG, "corrupt snapshot list table");
+    // Every live entry must name a vertex of the graph, carry no batch flag, and the lists must
+    // be strictly ascending: the kernels index by these ids and search these lists.
+    for (size_t i = 0; i < nmeta; i++) {
+        const uint32_t *l = pool.data() + meta[i].x;
+        for (uint32_t j = 0; j < meta[i].y; j++)
+            if ((l[j] >> 1) >= h.V || (l[j] & 1u) || (j && l[j] <= l[j - 1]))
+                return fail(CSM_ERR_INVALID_ARG, "corrupt snapshot adjacency list");
+    }
     const uint64_t max_batch = cfg_.max_batch ? cfg_.max_batch : (1ull << 20);
     unsigned long long want = cfg_.pool_entries ? cfg_.pool_entries : h.capacity;
     want = std::max<unsigned long long>(want, h.used + 64 * max_batch + (1u << 20));
