@@ -3,6 +3,7 @@ loudly (no fallback) when no GPU is present."""
 import ctypes
 import os
 import re
+import shutil
 import subprocess
 
 import pytest
@@ -107,3 +108,28 @@ def test_csmg_fails_loudly_without_gpu(tmp_path):
     assert p.returncode != 0
     assert "Read Graphs from Files" in p.stdout  # parsing ran, then the engine refused
     assert "no CUDA device" in p.stdout + p.stderr
+
+
+@pytest.mark.skipif(shutil.which("gcc") is None, reason="no C compiler")
+def test_ctypes_layouts_match_the_c_headers(tmp_path):
+    # Field offsets and struct sizes of the Python binding equal the C compiler's for every
+    # struct of include/csm.h and include/csm_server.h.
+    exe = str(tmp_path / "abi_layout")
+    subprocess.run(["gcc", "-std=c11", "-Wall", "-o", exe, os.path.join(ROOT, "tests", "native", "abi_layout.c"),
+                    "-I", os.path.join(ROOT, "include")], check=True)
+    out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split("\n")
+    types = {"csm_config": csm.CsmConfig, "csm_batch_result": csm.CsmBatchResult, "csm_stats": csm.CsmStats,
+             "csm_server_config": csm.CsmServerConfig, "csm_request_info": csm.CsmRequestInfo,
+             "csm_server_stats": csm.CsmServerStats}
+    checked = 0
+    for line in out:
+        if not line.strip():
+            continue
+        name, off = line.split()
+        a, b = name.split(".")
+        if a == "sizeof":
+            assert ctypes.sizeof(types[b]) == int(off), name
+        else:
+            assert getattr(types[a], b).offset == int(off), name
+        checked += 1
+    assert checked > 60
