@@ -230,10 +230,7 @@ def run_reference(args, w, world, rank):
         "metric": "incremental matches/sec", "value": value, "unit": "matches/s", "impl": "reference",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": f"{w.name}: Chung-Lu {len(w.data.vlabels)} vertices, {len(w.data.src)} initial edges;"
-                               f" step = one {w.batch_size}-update batch for one of {len(w.queries)} standing"
-                               " queries (stream, then its inverse)",
-                   "batch_size": w.batch_size, "queries": len(w.queries), "parallelism": "host threads"},
+        "config": workload_config(w, args, world),
         "cpu_baseline": {"value": value, "unit": "matches/s", "cores": threads, "kind": "port",
                          "sample": f"{args.steps} (query, batch) steps, each batch applied in full with counting "
                                    f"capped at {budget / args.steps:.1f} s per step: {items} seed items, "
@@ -241,6 +238,16 @@ def run_reference(args, w, world, rank):
         "e2e": {"value": value, "unit": "matches/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out))
+
+
+def workload_config(w, args, world):
+    """The `config` object of the JSON line; both arms print the same one."""
+    return {"workload": f"{w.name}: Chung-Lu {len(w.data.vlabels)} vertices, {len(w.data.src)} initial edges;"
+                        f" step = one {w.batch_size}-update batch for one of {len(w.queries)} standing"
+                        " queries (stream, then its inverse)",
+            "batch_size": w.batch_size, "queries": len(w.queries), "search_strategy": args.strategy,
+            "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (each engine's adjacency pool exceeds the 126 MB L2)"}
 
 
 def step_plan(w, count):
@@ -293,7 +300,7 @@ def run_ours(args, w, world, rank, local):
     for e in engines:
         e.reset_stats()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    matches, upd, lat = 0, 0, []
+    matches, upd, lat, dev_steps = 0, 0, [], []
     barrier(world)
     torch.cuda.synchronize(dev)
     with ClockSampler(local) as clk:
@@ -303,6 +310,7 @@ def run_ours(args, w, world, rank, local):
             matches += r.positive + r.negative
             upd += len(b.src)
             lat.append(r.latency_ns / 1e6)
+            dev_steps.append((r.positive, r.negative))
         ev1.record(stream)
         torch.cuda.synchronize(dev)
     barrier(world)
@@ -332,7 +340,7 @@ def run_ours(args, w, world, rank, local):
             h.numpy()[:] = dl
             arrs.append(h)
             pinned[id(b)] = arrs
-    matches_e2e, h2d = 0, 0
+    matches_e2e, h2d, e2e_steps = 0, 0, []
     barrier(world)
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
@@ -342,7 +350,13 @@ def run_ours(args, w, world, rank, local):
                                         l.numpy().view(np.uint32), dl.numpy()))[0]
         matches_e2e += r.positive + r.negative
         h2d += 13 * len(b.src)
+        e2e_steps.append((r.positive, r.negative))
     t_e2e = time.perf_counter() - t0
+    # Steps whose exact counts differ between the two runs (must be none).
+    Q, nb = len(w.queries), 2 * len(w.batches)
+    mismatched = [{"step": i, "query": qi, "stream_batch": ((args.warmup + i) // Q) % nb,
+                   "device": list(dev_steps[i]), "e2e": list(e2e_steps[i])}
+                  for i, (qi, b) in enumerate(timed) if dev_steps[i] != e2e_steps[i]]
     t_e2e_max = max_over_ranks(t_e2e, world, dev)
     pool_mb = max(st.pool_capacity for st in sts) * 4 / 2 ** 20
     for e in engines:
@@ -363,20 +377,20 @@ def run_ours(args, w, world, rank, local):
         "metric": "incremental matches/sec", "value": world * matches / tmax, "unit": "matches/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tmax / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": {"workload": f"{w.name}: Chung-Lu {len(w.data.vlabels)} vertices, {len(w.data.src)} initial edges;"
-                               f" step = one {w.batch_size}-update batch for one of {len(w.queries)} standing"
-                               " queries (stream, then its inverse)",
-                   "batch_size": w.batch_size, "queries": len(w.queries), "search_strategy": args.strategy,
-                   "parallelism": f"replicas x{world}",
-                   "l2": f"inputs larger than L2 (adjacency pool {pool_mb:.0f} MiB per engine, 126 MB L2)"},
+        "config": workload_config(w, args, world),
+        "adjacency_pool_mib_per_engine": pool_mb,
         "update_edges_per_s": world * upd / tmax,
         "p50_batch_ms": float(np.percentile(lat, 50)), "p99_batch_ms": float(np.percentile(lat, 99)),
         "matches_per_step": matches / args.steps,
         "e2e": {"value": world * matches_e2e / t_e2e_max, "unit": "matches/s",
                 "h2d_bytes_per_step": h2d // max(1, len(timed_e2e)), "d2h_bytes_per_step": 64,
                 "steps": "the timed steps again (state restored by their inverses)",
-                "counts_equal_to_device_run": matches_e2e == matches},
+                "counts_equal_to_device_run": matches_e2e == matches and not mismatched,
+                "mismatched_steps": mismatched},
         "gpu_launches": int(sum(st.kernel_launches for st in sts)),
+        "donation": {"items_donated": int(sum(st.donations for st in sts)),
+                     "refused_ring_full": int(sum(st.donations_refused for st in sts)),
+                     "compactions": int(sum(st.compactions for st in sts))},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": f"{peak_kind} hbm_gbs",
                      "kernel": "k_enumerate",

@@ -37,7 +37,8 @@ ERRORS = {
 EXPORTED = [
     "csm_default_config", "csm_create", "csm_destroy", "csm_load_query", "csm_load_graph",
     "csm_save_snapshot", "csm_load_snapshot",
-    "csm_apply_batch", "csm_apply_batch_device", "csm_apply_batch_device_static", "csm_get_edge_counts", "csm_get_embeddings",
+    "csm_apply_batch", "csm_apply_batch_device", "csm_apply_batch_device_static", "csm_set_time_limit",
+    "csm_get_edge_counts", "csm_get_embeddings",
     "csm_free", "csm_describe_plan", "csm_get_stats", "csm_reset_stats", "csm_device_memory",
     "csm_last_error", "csm_version",
 ]
@@ -71,6 +72,9 @@ class CsmConfig(ctypes.Structure):
         ("cuda_graphs", ctypes.c_int32),
         ("replan_drift_pct", ctypes.c_int32),
         ("semi_bfs_items_per_warp", ctypes.c_int32),
+        ("queue_slots", ctypes.c_int32),
+        ("reserved0", ctypes.c_int32),
+        ("time_limit_us", ctypes.c_uint64),
     ]
 
 
@@ -92,7 +96,7 @@ class CsmStats(ctypes.Structure):
         "batches", "enum_launches", "kernel_launches", "enum_scan_entries", "enum_probes",
         "enum_tail_lists", "donations", "enum_ns", "apply_ns", "pool_used", "pool_capacity",
         "compactions", "tuned_strategy", "tuned_steal_chunk", "tuned_warps_per_block", "tuned_occupancy",
-        "graph_launches", "replans")] + [("reserved", ctypes.c_uint64 * 2)]
+        "graph_launches", "replans", "donations_refused")] + [("reserved", ctypes.c_uint64 * 1)]
 
 
 class CsmError(RuntimeError):
@@ -152,6 +156,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.csm_apply_batch_device.argtypes = [vp, ctypes.c_uint64, vp, vp, vp, vp, vp, ctypes.POINTER(CsmBatchResult)]
     lib.csm_apply_batch_device_static.argtypes = [vp, ctypes.c_uint64, vp, vp, vp, vp, vp,
                                                   ctypes.POINTER(CsmBatchResult)]
+    lib.csm_set_time_limit.argtypes = [vp, ctypes.c_uint64]
     lib.csm_get_edge_counts.argtypes = [vp, ctypes.c_int32, u64p, u64p, ctypes.c_uint32, u32p]
     lib.csm_get_embeddings.argtypes = [vp, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(u32p), u64p]
     lib.csm_free.argtypes = [vp]
@@ -310,6 +315,24 @@ class Engine:
             self._h, n, ctypes.c_void_p(src_ptr), ctypes.c_void_p(dst_ptr), ctypes.c_void_p(lab_ptr),
             ctypes.c_void_p(del_ptr) if del_ptr else None, ctypes.c_void_p(stream) if stream else None, out))
         return list(out)[: len(self.queries)]
+
+    def set_time_limit(self, us: int):
+        """csm_set_time_limit: enumeration launches of later batches stop after `us` microseconds."""
+        self._check(self.lib.csm_set_time_limit(self._h, us))
+
+    def apply_partial(self, b: Batch):
+        """Like apply(), but returns (status, results): CSM_ERR_TIMEOUT comes back with the partial
+        counts instead of raising."""
+        s, d, l = _u32(b.src), _u32(b.dst), _u32(b.elabels)
+        out = (CsmBatchResult * max(1, len(self.queries)))()
+        dp = None
+        if b.is_delete is not None:
+            dl = np.ascontiguousarray(np.asarray(b.is_delete, dtype=np.uint8))
+            dp = _ptr(dl, ctypes.c_uint8)
+        rc = self.lib.csm_apply_batch(self._h, len(s), _ptr(s), _ptr(d), _ptr(l), dp, out)
+        if rc not in (CSM_OK, -4):
+            self._check(rc)
+        return rc, list(out)[: len(self.queries)]
 
     def edge_counts(self, qid: int):
         n = ctypes.c_uint32()

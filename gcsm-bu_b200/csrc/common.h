@@ -103,24 +103,46 @@ struct WorkItem {
 };
 
 // Device-side control block of one enumeration launch.
+//
+// The donation queue is a ring of `qcap` (a power of two, at least 32) slots addressed by
+// monotone 32-bit positions: position p lives in slot p & (qcap - 1).  Each slot carries a
+// 64-bit sequence word (epoch << 32 | position): the producer of position p may write the slot
+// once its word reads (epoch, p) — or, in the first lap, any older epoch — and publishes with
+// (epoch, p + 1); the consumer that takes p releases the slot with (epoch, p + qcap).  Slots are
+// reused for the whole launch, no position is ever skipped, and nobody waits on a slot.
 struct EnumControl {
     unsigned long long ticket;        // next seed / frontier ticket
     unsigned long long nticket;       // total tickets
-    unsigned int q_write;             // donation slots reserved
-    unsigned int q_read;              // donation slots claimed
+    unsigned int q_head;              // donation positions reserved
+    unsigned int q_tail;              // donation positions claimed
     unsigned int hungry;              // outstanding work requests of idle warps
     unsigned int active;              // warps holding work
-    unsigned int error;               // bit 0 timeout, bit 1 output overflow, bit 2 queue overflow
-    unsigned int epoch;               // launch epoch, marks ready slots
+    unsigned int error;               // CSM_ERRBIT_* of this launch
+    unsigned int epoch;               // launch epoch, stamps the queue's sequence words
     unsigned long long out_rows;      // rows written (materialize / expand)
     unsigned long long scan_entries;  // statistics
     unsigned long long probes;
     unsigned long long tail_lists;
     unsigned long long donations;
     unsigned long long expand_bound;  // upper bound of the next BFS level
+    unsigned long long t_start;       // device clock (ns) when the launch's control block was reset
+    unsigned long long queue_full;    // donations refused because the ring was full
+    // First failed consistency check of the launch (CSM_ERRBIT_CORRUPT): where (CSM_BAD_*) and
+    // three values describing it.  The offending item, list or entry is skipped, not used.
+    unsigned int bad_where;
+    unsigned int bad_a, bad_b, bad_c;
 };
 
-#define CSM_ERRBIT_TIMEOUT 1u
+#define CSM_BAD_ITEM 1u      // a claimed work item: a = plan, b = depth, c = ring position
+#define CSM_BAD_FRONTIER 2u  // a frontier item: a = plan, b = depth, c = ticket
+#define CSM_BAD_LIST 3u      // a list-table entry past the pool: a = offset, b = size, c = level
+#define CSM_BAD_ENTRY 4u     // an adjacency entry naming no vertex: a = entry, b = offset, c = level
+
+// Positions past this are never reserved (a launch would need 2^31 donations to reach it).
+#define CSM_QUEUE_POS_LIMIT 0x7FFFFFFFu
+#define CSM_QUEUE_MIN_SLOTS 32u
+
+#define CSM_ERRBIT_TIMEOUT 1u  // the launch ran past its time limit and stopped early
 #define CSM_ERRBIT_OUTPUT 2u
-#define CSM_ERRBIT_QUEUE 4u
 #define CSM_ERRBIT_POOL 8u
+#define CSM_ERRBIT_CORRUPT 16u  // a consistency check failed (see EnumControl.bad_*)

@@ -109,6 +109,12 @@ csm_status csm_apply_batch_device(csm_engine *e, uint64_t n, const uint32_t *d_s
     });
 }
 
+csm_status csm_set_time_limit(csm_engine *e, uint64_t time_limit_us) {
+    if (!e) return CSM_ERR_INVALID_ARG;
+    e->impl.set_time_limit_us(time_limit_us);
+    return CSM_OK;
+}
+
 csm_status csm_get_edge_counts(const csm_engine *e, int32_t query_id, uint64_t *positive, uint64_t *negative,
                                uint32_t capacity, uint32_t *n_edges_out) {
     if (!e) return CSM_ERR_INVALID_ARG;

@@ -24,6 +24,16 @@ cudaError_t dalloc(T **p, size_t count) {
 
 }  // namespace
 
+// One-line description of a failed device consistency check (EnumControl.bad_*).
+static std::string describe_bad(const EnumControl &c) {
+    static const char *what[] = {"?", "claimed work item (plan, depth, ring position)",
+                                 "frontier item (plan, depth, ticket)", "list-table entry (offset or vertex, size or relation, level)",
+                                 "adjacency entry (entry, pool index, level)"};
+    const uint32_t w = c.bad_where < 5 ? c.bad_where : 0;
+    return std::string("device consistency check failed: ") + what[w] + " = (" + std::to_string(c.bad_a) + ", " +
+           std::to_string(c.bad_b) + ", " + std::to_string(c.bad_c) + "); the batch was abandoned";
+}
+
 Options resolve_options(const csm_config &cfg) {
     Options o;
     switch (cfg.algorithm) {
@@ -97,6 +107,15 @@ csm_status Engine::init() {
     sm_count_ = prop.multiProcessorCount;
     CSM_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
     for (auto &e : ev_) CSM_CUDA(cudaEventCreate(&e));
+    if (cfg_.queue_slots != 0) {
+        const uint32_t q = (uint32_t)cfg_.queue_slots;
+        if (cfg_.queue_slots < (int32_t)CSM_QUEUE_MIN_SLOTS || cfg_.queue_slots > (1 << 24) || (q & (q - 1)) != 0)
+            return fail(CSM_ERR_INVALID_ARG, "queue_slots must be a power of two in [32, 2^24]");
+        qcap_ = q;
+    } else {
+        qcap_ = 1u << 18;
+    }
+    time_limit_us_ = cfg_.time_limit_us;
     warps_per_block_ = cfg_.warps_per_block > 0 && cfg_.warps_per_block <= 8 ? cfg_.warps_per_block : 8;
     LaunchConfig lc;
     lc.strategy = opt_.search_strategy;
@@ -157,7 +176,7 @@ Engine::~Engine() {
     void *dev[] = {d_elab_raw_, d_rel_table_, d_spec_begin_, d_specs_, d_bits_, g_.meta, g_.cap, g_.pool, g_.pool_top,
                    g_.vlab, d_plans_, d_terms_, d_upd_src_, d_upd_dst_, d_upd_lab_, d_upd_del_, d_keys_raw_, d_keys_,
                    d_sort_temp_, bs_.eff, bs_.heads, bs_.nheads, bs_.seg_nins, bs_.seg_ndel, bs_.seg_end, bs_.scr_y,
-                   bs_.scr_lb, bs_.counters, bs_.error, d_ctrl_, d_queue_, d_ready_, d_seed_lo_, d_ticket_prefix_,
+                   bs_.scr_lb, bs_.counters, bs_.error, d_ctrl_, d_queue_, d_seq_, d_seed_lo_, d_ticket_prefix_,
                    d_counts_, d_frontier_[0], d_frontier_[1], d_rows_, d_misc_, d_rel_delta_, d_touched_};
     for (void *p : dev)
         if (p) cudaFree(p);
@@ -397,14 +416,14 @@ csm_status Engine::finish_load() {
     cudaFreeHost(h_counts_);
     h_counts_ = nullptr;
     CSM_CUDA(cudaMallocHost(&h_counts_, sizeof(unsigned long long) * (2 * np + 32)));
-    // Donation queue and the semi-BFS frontier.
-    qcap_ = 1u << 21;
+    // Donation ring and the semi-BFS frontier.  The ring's slots are reused for the whole
+    // launch, so it only needs room for the items in flight at once.
     CSM_CUDA(dalloc(&d_queue_, qcap_));
-    CSM_CUDA(dalloc(&d_ready_, qcap_));
-    CSM_CUDA(cudaMemset(d_ready_, 0, sizeof(uint32_t) * qcap_));
+    CSM_CUDA(dalloc(&d_seq_, qcap_));
+    CSM_CUDA(cudaMemset(d_seq_, 0, sizeof(unsigned long long) * qcap_));
     sc_.ctrl = d_ctrl_;
     sc_.queue = d_queue_;
-    sc_.ready = d_ready_;
+    sc_.seq = d_seq_;
     sc_.qcap = qcap_;
     sc_.seed_lo = d_seed_lo_;
     sc_.ticket_prefix = d_ticket_prefix_;
@@ -790,6 +809,15 @@ csm_status Engine::apply_device_noalloc(uint64_t n, const uint32_t *src, const u
         return fail(CSM_ERR_LIMIT, "batch of " + std::to_string(n) + " updates exceeds the " +
                                        std::to_string(batch_cap_) +
                                        " preallocated at load time (csm_config.max_batch); this call does not grow it");
+    // This call never compacts or grows the adjacency pool: refuse, before anything changes, a
+    // batch that could need more room than is free (the headroom compaction keeps elsewhere).
+    const unsigned long long headroom = 64ull * n + (1u << 20);
+    if (stats_.pool_used + headroom > g_.pool_cap)
+        return fail(CSM_ERR_LIMIT, "the adjacency pool has " + std::to_string(g_.pool_cap - std::min<unsigned long long>(
+                                                                                      stats_.pool_used, g_.pool_cap)) +
+                                       " free entries, fewer than the " + std::to_string(headroom) +
+                                       " this batch may need; this call never compacts the pool: apply a batch "
+                                       "through csm_apply_batch_device, or size pool_entries for the stream");
     cudaStream_t s = stream ? stream : stream_;
     CSM_CUDA(cudaEventRecord(ev_[0], s));
     const EnumScratch saved = sc_;
@@ -932,6 +960,7 @@ csm_status Engine::run_batch(uint64_t n, const uint32_t *src, const uint32_t *ds
     rows_valid_ = false;
     phase_ran_[0] = phase_ran_[1] = false;
     last_frontier_rows_ = 0;
+    deferred_ = CSM_OK;
     NlfTables nt{d_spec_begin_, d_specs_, d_bits_, words_};
     const bool tuning = tune_left_ > 0 && !no_alloc_ && cfg_.materialize_rows == 0;
     csm_status est;
@@ -939,7 +968,12 @@ csm_status Engine::run_batch(uint64_t n, const uint32_t *src, const uint32_t *ds
         est = launch_graph(n, has_delete, s);
     else
         est = enqueue_batch(n, src, dst, elabel, is_delete, has_delete, tuning, s);
-    if (est != CSM_OK) return est;
+    if (est != CSM_OK) {
+        // The batch's device work stopped part way (a CUDA failure): the graph may hold part
+        // of it, so the engine refuses later batches.
+        poisoned_ = true;
+        return est;
+    }
     unsigned int *h_err = reinterpret_cast<unsigned int *>(h_counts_ + 2 * np + 3);
     for (int attempt = 0;; attempt++) {
         if (attempt > 0) {
@@ -999,8 +1033,18 @@ csm_status Engine::run_batch(uint64_t n, const uint32_t *src, const uint32_t *ds
         stats_.enum_probes += c.probes;
         stats_.enum_tail_lists += c.tail_lists;
         stats_.donations += c.donations;
-        if (c.error & CSM_ERRBIT_TIMEOUT) return fail(CSM_ERR_TIMEOUT, "enumeration wait bound exceeded");
-        if (c.error & CSM_ERRBIT_OUTPUT) return fail(CSM_ERR_OVERFLOW, "embedding row buffer too small");
+        stats_.donations_refused += c.queue_full;
+        if (c.error & CSM_ERRBIT_CORRUPT) {
+            poisoned_ = true;
+            return fail(CSM_ERR_STATE, describe_bad(c));
+        }
+        // A launch that ran past its time limit stopped early; the graph still holds the whole
+        // batch (the update kernels do not depend on the counts), so only the counts are short.
+        if ((c.error & CSM_ERRBIT_TIMEOUT) && deferred_ == CSM_OK)
+            deferred_ = fail(CSM_ERR_TIMEOUT, "the enumeration ran past its time limit (time_limit_us): this batch's "
+                                              "counts are incomplete; the graph holds the whole batch");
+        if ((c.error & CSM_ERRBIT_OUTPUT) && deferred_ == CSM_OK)
+            deferred_ = fail(CSM_ERR_OVERFLOW, "embedding row buffer too small");
     }
     for (uint32_t i = 0; i < 2 * np; i++) last_counts_[i] = h_counts_[i];
     const uint64_t ins = h_counts_[2 * np], del = h_counts_[2 * np + 1];
@@ -1022,13 +1066,14 @@ csm_status Engine::run_batch(uint64_t n, const uint32_t *src, const uint32_t *ds
             r.apply_ns = r.latency_ns > r.enum_ns ? r.latency_ns - r.enum_ns : 0;
         }
     }
-    if (cfg_.materialize_rows) rows_valid_ = true;
-    if (no_alloc_) return CSM_OK;
+    if (cfg_.materialize_rows) rows_valid_ = deferred_ == CSM_OK;
+    if (no_alloc_) return deferred_;
     if (d_rel_delta_ && m) {
         const csm_status rst = maybe_replan();
         if (rst != CSM_OK) return rst;
     }
-    return maybe_compact(s);
+    const csm_status cst = maybe_compact(s);
+    return cst != CSM_OK ? cst : deferred_;
 }
 
 csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
@@ -1050,15 +1095,15 @@ csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
     P.seed_lo = sc_.seed_lo;
     P.ticket_prefix = sc_.ticket_prefix;
     P.queue = sc_.queue;
-    P.ready = sc_.ready;
-    P.qcap = sc_.qcap;
+    P.seq = sc_.seq;
+    P.qmask = sc_.qcap - 1;
     P.ctrl = sc_.ctrl;
     P.counts = d_counts_ + (phase == CSM_PHASE_INS ? np : 0);
     P.steal_min = lc_.steal_chunk;
-    // An idle warp leaves as soon as no warp holds work; the bound (about a minute of
-    // polling) only ends the wait if that never happens.
+    // An idle warp leaves as soon as no warp holds work; the bound (seconds of polling) only
+    // ends the wait if that never happens.
     P.idle_limit = 1u << 24;
-    P.ready_limit = 1u << 22;
+    P.time_limit_ns = time_limit_us_ * 1000ull;
     P.abort_flag = phase == CSM_PHASE_INS ? bs_.error : nullptr;
     P.touched = d_touched_;
     P.rows = d_rows_;
@@ -1113,7 +1158,14 @@ csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
             CSM_CUDA(cudaStreamSynchronize(s));
             const unsigned long long rows_out = h_ctrl_[ph].out_rows;
             const unsigned int errb = h_ctrl_[ph].error;
-            if (errb & CSM_ERRBIT_OUTPUT) return fail(CSM_ERR_OVERFLOW, "semi-BFS frontier overflow");
+            if (errb & (CSM_ERRBIT_OUTPUT | CSM_ERRBIT_TIMEOUT | CSM_ERRBIT_CORRUPT)) {
+                // Out of time (or, never expected, of frontier room): the phase stops here and
+                // the batch reports it; the update kernels after it still run.
+                if ((errb & CSM_ERRBIT_OUTPUT) && deferred_ == CSM_OK)
+                    deferred_ = fail(CSM_ERR_OVERFLOW, "semi-BFS frontier overflow");
+                CSM_CUDA(record_event(ev_[3 + 2 * ph], s));
+                return CSM_OK;
+            }
             const bool grew = rows_out != nfront || frontier == nullptr;
             frontier = d_frontier_[buf];
             nfront = rows_out;
@@ -1143,7 +1195,7 @@ csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
         // Collect rows per query for csm_get_embeddings (a validation path: synchronous).
         CSM_CUDA(cudaStreamSynchronize(s));
         const EnumControl &c = h_ctrl_[ph];
-        if (c.error & CSM_ERRBIT_OUTPUT) return fail(CSM_ERR_OVERFLOW, "embedding row buffer too small");
+        if (c.error & (CSM_ERRBIT_OUTPUT | CSM_ERRBIT_TIMEOUT)) return CSM_OK;  // reported by run_batch
         const unsigned long long nr = c.out_rows;
         std::vector<uint32_t> h(nr * CSM_ROW_WORDS);
         if (nr) CSM_CUDA(cudaMemcpy(h.data(), d_rows_, sizeof(uint32_t) * h.size(), cudaMemcpyDeviceToHost));
@@ -1163,35 +1215,46 @@ csm_status Engine::maybe_compact(cudaStream_t s) {
     const uint64_t max_batch = batch_cap_ ? batch_cap_ : 65536;
     const unsigned long long headroom = 64ull * max_batch + (1u << 20);
     if (used + headroom < g_.pool_cap && used < g_.pool_cap / 4 * 3) return CSM_OK;
-    // Lay every list out again with fresh slack; grow the pool when the live lists need it.
-    unsigned long long new_cap = g_.pool_cap;
-    for (int attempt = 0; attempt < 4; attempt++) {
-        uint32_t *np = nullptr;
-        cudaError_t e = cudaMalloc(&np, sizeof(uint32_t) * new_cap);
-        if (e != cudaSuccess) return cuda_fail(e, "pool compaction");
-        unsigned long long live = 0;
-        e = store_compact(g_, np, new_cap, s, live);
-        if (e == cudaSuccess && live + headroom < new_cap && live < new_cap / 4 * 3) {
-            cudaFree(g_.pool);
-            g_.pool = np;
-            g_.pool_cap = new_cap;
-            clear_graphs();
-            graph_gen_++;
-            stats_.pool_used = live;
-            stats_.pool_capacity = new_cap;
-            stats_.compactions++;
-            return CSM_OK;
-        }
-        cudaFree(np);
-        if (e != cudaSuccess && e != cudaErrorMemoryAllocation) return cuda_fail(e, "pool compaction");
-        if (e == cudaSuccess) {
-            // The layout fit but left too little headroom: keep it only if growth is impossible.
-            new_cap = std::min<unsigned long long>(0xFFFFFFF0ull, std::max(new_cap * 2, 2 * (live + headroom)));
-        } else {
-            new_cap = std::min<unsigned long long>(0xFFFFFFF0ull, new_cap * 2);
-        }
+    // Lay every list out again with fresh slack, growing the pool when the live lists leave too
+    // little room.  The layout is computed first; the graph changes only once a pool for it has
+    // been allocated, so a failure here leaves the current layout intact.
+    unsigned long long *offsets = nullptr, total = 0;
+    cudaError_t e = store_layout(g_, &offsets, total, s);
+    if (e != cudaSuccess) return cuda_fail(e, "pool compaction layout");
+    const unsigned long long limit = 0xFFFFFFF0ull;
+    auto roomy = [&](unsigned long long cap) { return total + headroom < cap && total < cap / 4 * 3; };
+    unsigned long long want = g_.pool_cap;
+    if (!roomy(want)) want = std::min(limit, std::max(want * 2, 2 * (total + headroom)));
+    uint32_t *np = nullptr;
+    e = total <= want ? cudaMalloc(&np, sizeof(uint32_t) * want) : cudaErrorMemoryAllocation;
+    if (e == cudaErrorMemoryAllocation && want > g_.pool_cap && total <= g_.pool_cap) {
+        // No memory to grow: a same-size pool still recovers the slack of relocated lists.
+        cudaGetLastError();
+        want = g_.pool_cap;
+        e = cudaMalloc(&np, sizeof(uint32_t) * want);
     }
-    return fail(CSM_ERR_OOM, "adjacency pool cannot grow further");
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(offsets);
+        return fail(CSM_ERR_OOM, "adjacency pool cannot be compacted: the live lists need " + std::to_string(total) +
+                                     " entries");
+    }
+    e = store_relayout(g_, np, offsets, total, s);
+    cudaFree(offsets);
+    if (e != cudaSuccess) {
+        cudaFree(np);
+        poisoned_ = true;
+        return cuda_fail(e, "pool compaction");
+    }
+    cudaFree(g_.pool);
+    g_.pool = np;
+    g_.pool_cap = want;
+    clear_graphs();
+    graph_gen_++;
+    stats_.pool_used = total;
+    stats_.pool_capacity = want;
+    stats_.compactions++;
+    return CSM_OK;
 }
 
 csm_status Engine::edge_counts(int32_t qid, uint64_t *pos, uint64_t *neg, uint32_t capacity, uint32_t *n_out) const {

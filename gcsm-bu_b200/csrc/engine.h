@@ -18,13 +18,13 @@
 
 namespace csm {
 
-// Scratch of the enumeration kernel: control block, donation queue with its ready flags, and
+// Scratch of the enumeration kernel: control block, donation ring with its sequence words, and
 // the per-plan seed ranges and ticket prefixes (3 * nplans and nplans + 1 words).
 struct EnumScratch {
     EnumControl *ctrl = nullptr;
     WorkItem *queue = nullptr;
-    uint32_t *ready = nullptr;
-    uint32_t qcap = 0;
+    unsigned long long *seq = nullptr;  // per-slot sequence words of the donation ring
+    uint32_t qcap = 0;                  // ring slots (a power of two, >= CSM_QUEUE_MIN_SLOTS)
     uint32_t *seed_lo = nullptr;
     uint32_t *ticket_prefix = nullptr;
 };
@@ -97,6 +97,22 @@ class Engine {
     // Frontier items at which the dynamic semi-BFS stops expanding.
     uint64_t semi_bfs_target_items() const { return (uint64_t)lc_.frontier_mult * enum_warps(); }
     uint64_t batch_capacity() const { return batch_cap_; }
+    // Device address of the library's static scratch array for this engine, looked up with
+    // `lookup` on the first call (the engine's device current).  Kept per engine: an engine
+    // lives in one device context, while a context re-created after cudaDeviceReset may place
+    // the array elsewhere.
+    cudaError_t static_scratch(cudaError_t (*lookup)(void **), void **out) {
+        if (!static_scratch_) {
+            void *p = nullptr;
+            const cudaError_t rc = lookup(&p);
+            if (rc != cudaSuccess) return rc;
+            static_scratch_ = p;
+        }
+        *out = static_scratch_;
+        return cudaSuccess;
+    }
+    // Enumeration time limit for later batches (microseconds per launch, 0 = none).
+    void set_time_limit_us(uint64_t us) { time_limit_us_ = us; }
     int device() const { return device_; }
     cudaStream_t stream() const { return stream_; }
     csm_status edge_counts(int32_t qid, uint64_t *pos, uint64_t *neg, uint32_t capacity, uint32_t *n_out) const;
@@ -167,8 +183,10 @@ class Engine {
     // Enumeration state.
     EnumControl *d_ctrl_ = nullptr;
     WorkItem *d_queue_ = nullptr;
-    uint32_t *d_ready_ = nullptr;
+    unsigned long long *d_seq_ = nullptr;
     uint32_t qcap_ = 0;
+    uint64_t time_limit_us_ = 0;              // per enumeration launch; 0 = none
+    csm_status deferred_ = CSM_OK;            // timeout / overflow of this batch, reported at its end
     unsigned long long last_frontier_rows_ = 0;
     // CUDA graphs of whole batches (depth-first strategies), keyed by what the capture bakes in.
     struct GraphKey {
@@ -237,6 +255,7 @@ class Engine {
     bool phase_ran_[2] = {false, false};
     EnumScratch sc_;                          // scratch used by enumerate_phase
     bool no_alloc_ = false;                   // inside apply_device_noalloc
+    void *static_scratch_ = nullptr;          // see static_scratch()
     int warps_per_block_ = 8;
     int occupancy_ = 4;                       // enumeration kernel variant (blocks per SM)
     int blocks_ = 0;

@@ -84,6 +84,31 @@ __device__ __forceinline__ const uint32_t *bitmap(const EnumParams &P, uint32_t 
     return P.bits + (size_t)id * P.words;
 }
 
+// Records the launch's first failed consistency check (the caller skips what failed it).
+__device__ void record_bad(const EnumParams &P, uint32_t where, uint32_t a, uint32_t b, uint32_t c) {
+    if (atomicCAS(&P.ctrl->bad_where, 0u, where) == 0u) {
+        P.ctrl->bad_a = a;
+        P.ctrl->bad_b = b;
+        P.ctrl->bad_c = c;
+    }
+    atomicOr(&P.ctrl->error, CSM_ERRBIT_CORRUPT);
+}
+
+// {offset, size} of list (rel, v), checked against the vertex range and the pool; a list that
+// fails is recorded and read as empty.
+__device__ __forceinline__ uint2 list_of(const EnumParams &P, uint32_t rel, uint32_t v, uint32_t level) {
+    if (v >= P.g.V || rel >= P.g.R) {
+        record_bad(P, CSM_BAD_LIST, v, rel, 0x80000000u | level);
+        return make_uint2(0u, 0u);
+    }
+    const uint2 ms = __ldg(P.g.meta + (size_t)rel * P.g.V + v);
+    if ((unsigned long long)ms.x + ms.y > P.g.pool_cap) {
+        record_bad(P, CSM_BAD_LIST, ms.x, ms.y, level);
+        return make_uint2(0u, 0u);
+    }
+    return ms;
+}
+
 // First index in [lo, hi) of the sorted list L whose entry is >= key2, found by the whole warp
 // with 32-ary search: each round reads 32 evenly spaced entries and keeps the bracket that
 // holds the answer, so a list of n entries costs about log32(n) dependent reads.
@@ -134,7 +159,7 @@ __device__ void prep_tail_shared(WarpState &S, const EnumParams &P, const DevPla
             const uint32_t rel = __ldg(&T->key_rel[lane]);
             const bool old = __ldg(&T->key_old[lane]) != 0;
             const uint32_t x = S.f[pd];
-            const uint2 ms = __ldg(P.g.meta + (size_t)rel * P.g.V + x);
+            const uint2 ms = list_of(P, rel, x, 100 + d);
             uint32_t left = ms.y - (old ? flagged_in_list(P, rel, x) : 0u);
             const uint32_t excl = __ldg(&T->key_excl[lane]);
             for (uint32_t j = 0; j < d; j++) {
@@ -174,7 +199,7 @@ __device__ unsigned long long tail_count_lane(const WarpState &S, const EnumPara
             (void)old;
         } else {
             const uint32_t x = (pd == d) ? v : x0;  // d >= 2: pd == d; d == 1: parent 0 or 1
-            const uint2 ms = __ldg(P.g.meta + (size_t)rel * P.g.V + x);
+            const uint2 ms = list_of(P, rel, x, 200 + d);
             left = ms.y - (old ? flagged_in_list(P, rel, x) : 0u);
             const uint32_t excl = __ldg(&T->key_excl[k]);
             for (uint32_t j = 0; j <= d; j++) {
@@ -223,7 +248,7 @@ __device__ void enter_level(WarpState &S, const EnumParams &P, const DevPlan *pl
         const uint32_t rel = __ldg(&lv->bn_rel[lane]);
         const uint32_t dep = __ldg(&lv->bn_depth[lane]);
         const uint32_t v = S.f[dep];
-        const uint2 ms = __ldg(P.g.meta + (size_t)rel * P.g.V + v);
+        const uint2 ms = list_of(P, rel, v, d);
         const uint32_t slot = __ldg(&lv->bn_base) + lane;
         S.poff[slot] = ms.x;
         S.psz[slot] = ms.y;
@@ -260,7 +285,7 @@ __device__ unsigned long long tail_count(WarpState &S, const EnumParams &P, cons
     if (lane < nkeys) {
         const uint32_t rel = __ldg(&T->key_rel[lane]);
         const uint32_t x = S.f[__ldg(&T->key_parent[lane])];
-        const uint2 ms = __ldg(P.g.meta + (size_t)rel * P.g.V + x);
+        const uint2 ms = list_of(P, rel, x, 300 + E);
         S.t_off[lane] = ms.x;
         S.t_size[lane] = ms.y;
         // Flagged entries of this list = batch edges of (rel, x) in this phase.
@@ -303,6 +328,10 @@ __device__ unsigned long long tail_count(WarpState &S, const EnumParams &P, cons
                     const uint32_t e = __ldg(P.g.pool + S.t_off[k0] + idx);
                     w = e >> 1;
                     ok = !(old0 && (e & 1u));
+                    if (w >= P.g.V) {
+                        record_bad(P, CSM_BAD_ENTRY, e, S.t_off[k0] + idx, 700 + E);
+                        ok = false;
+                    }
                 }
                 for (uint32_t z = 0; ok && z < E; z++) ok = S.f[z] != w;
                 for (uint32_t k = 0; ok && k < nkeys; k++) {
@@ -339,31 +368,64 @@ __device__ unsigned long long tail_count(WarpState &S, const EnumParams &P, cons
     return total;
 }
 
-// Reserves `cnt` queue slots; returns the first slot or 0xFFFFFFFF when the queue is full.
-// Slots that were reserved past a failed reservation are filled with null items.
-__device__ uint32_t reserve_slots(const EnumParams &P, uint32_t cnt) {
-    const uint32_t lane = lane_id();
-    uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(&P.ctrl->q_write, cnt);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    if (base + cnt <= P.qcap) return base;
-    // Mark the reachable part as null so that consumers skip it.
-    for (uint32_t s = base; s < P.qcap && s < base + cnt; s++) {
-        if (lane == 0) {
-            P.queue[s].depth = 0xFFFFFFFFu;
-            __threadfence();
-            atomicExch(P.ready + s, P.ctrl->epoch);
-        }
-    }
-    __syncwarp();
-    return 0xFFFFFFFFu;  // a full queue only costs balance: the donor keeps the work
+__device__ __forceinline__ unsigned long long slot_stamp(uint32_t epoch, uint32_t pos) {
+    return ((unsigned long long)epoch << 32) | pos;
 }
 
-__device__ void publish_item(const EnumParams &P, uint32_t slot, uint32_t plan, uint32_t depth, uint32_t lo,
+__device__ __forceinline__ unsigned long long device_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Checks the work item copied into S: plan, depth, candidate range and prefix vertex ids.  A
+// failing item is recorded (`where`, `tag`) and must be skipped.  Warp-uniform.
+__device__ bool item_ok(const WarpState &S, const EnumParams &P, uint32_t where, uint32_t tag) {
+    const uint32_t lane = lane_id();
+    const uint32_t plan = S.item_plan, depth = S.item_depth;
+    bool ok = plan < P.nplans;
+    if (ok) {
+        if (depth == 0) ok = S.item_lo < S.item_hi && S.item_hi <= P.m;
+        else ok = depth >= 2 && depth < P.plans[plan].n && S.item_lo <= S.item_hi;
+    }
+    const bool fok = !ok || lane >= depth || S.f[lane] < P.g.V;
+    ok = __all_sync(0xffffffffu, ok && fok);
+    if (!ok && lane == 0) record_bad(P, where, plan, depth, tag);
+    __syncwarp();
+    return ok;
+}
+
+// Reserves `cnt` (1..32) consecutive ring positions; returns the first, or 0xFFFFFFFF when the
+// ring has no room (a full ring only costs balance: the donor keeps its work).  A position p of
+// a later lap is free once the consumer of p - qcap has released its slot with stamp (epoch, p);
+// first-lap positions are free as soon as nobody has reserved them.
+__device__ uint32_t reserve_slots(const EnumParams &P, uint32_t cnt) {
+    const uint32_t lane = lane_id();
+    const uint32_t ep = P.ctrl->epoch;
+    for (int tries = 0; tries < 16; tries++) {
+        uint32_t pos = 0;
+        if (lane == 0) pos = *(volatile unsigned int *)&P.ctrl->q_head;
+        pos = __shfl_sync(0xffffffffu, pos, 0);
+        if (pos > CSM_QUEUE_POS_LIMIT - cnt) break;
+        const uint32_t p = pos + lane;
+        bool free_slot = true;
+        if (lane < cnt && p > P.qmask)
+            free_slot = *(volatile unsigned long long *)(P.seq + (p & P.qmask)) == slot_stamp(ep, p);
+        if (!__all_sync(0xffffffffu, free_slot)) break;
+        uint32_t won = 0;
+        if (lane == 0) won = atomicCAS(&P.ctrl->q_head, pos, pos + cnt) == pos;
+        if (__shfl_sync(0xffffffffu, won, 0)) return pos;
+    }
+    if (lane == 0) atomicAdd(&P.ctrl->queue_full, 1ull);
+    return 0xFFFFFFFFu;
+}
+
+// Writes the item of ring position `pos` and publishes it with stamp (epoch, pos + 1).
+__device__ void publish_item(const EnumParams &P, uint32_t pos, uint32_t plan, uint32_t depth, uint32_t lo,
                              uint32_t hi, const uint32_t *prefix, uint32_t nprefix, bool extra, uint32_t extra_v,
                              uint32_t extra_pos) {
     const uint32_t lane = lane_id();
-    WorkItem *it = P.queue + slot;
+    WorkItem *it = P.queue + (pos & P.qmask);
     if (lane == 0) {
         it->plan = plan;
         it->depth = depth;
@@ -374,7 +436,7 @@ __device__ void publish_item(const EnumParams &P, uint32_t slot, uint32_t plan, 
     if (extra && lane == 0) it->f[extra_pos] = extra_v;
     __threadfence();
     __syncwarp();
-    if (lane == 0) atomicExch(P.ready + slot, P.ctrl->epoch);
+    if (lane == 0) atomicExch(P.seq + (pos & P.qmask), slot_stamp(P.ctrl->epoch, pos + 1));
     __syncwarp();
 }
 
@@ -425,41 +487,32 @@ __device__ bool try_donate(WarpState &S, const EnumParams &P, const DevPlan *pl,
     return false;
 }
 
-// Claims one donated item into S; returns 1 on success, 0 if the queue is empty.
-__device__ int claim_item(WarpState &S, const EnumParams &P, unsigned int &err) {
+// Claims the oldest published item into S; returns 1 on success, 0 when none is ready.  The
+// position at the ring's tail is taken only once its item is published, so a claim never waits;
+// after copying the item the slot is released for the position one lap later.
+__device__ int claim_item(WarpState &S, const EnumParams &P) {
     const uint32_t lane = lane_id();
-    uint32_t slot = 0xFFFFFFFFu;
+    const uint32_t ep = P.ctrl->epoch;
+    uint32_t pos = 0xFFFFFFFFu;
     if (lane == 0) {
-        volatile unsigned int *qr = &P.ctrl->q_read;
-        volatile unsigned int *qw = &P.ctrl->q_write;
-        for (int tries = 0; tries < 256; tries++) {
-            const unsigned int r = *qr;
-            unsigned int w = *qw;
-            if (w > P.qcap) w = P.qcap;
-            if (r >= w) break;
-            if (atomicCAS(&P.ctrl->q_read, r, r + 1) == r) {
-                slot = r;
+        volatile unsigned int *qt = &P.ctrl->q_tail;
+        for (int tries = 0; tries < 64; tries++) {
+            const uint32_t t = *qt;
+            const unsigned long long sq = *(volatile unsigned long long *)(P.seq + (t & P.qmask));
+            if (sq != slot_stamp(ep, t + 1)) {
+                if (*qt == t) break;  // the tail's item is not published yet: nothing ready
+                continue;             // another warp took it; look at the new tail
+            }
+            if (atomicCAS(&P.ctrl->q_tail, t, t + 1) == t) {
+                pos = t;
                 break;
             }
         }
-        if (slot != 0xFFFFFFFFu) {
-            volatile uint32_t *rd = P.ready + slot;
-            const uint32_t ep = P.ctrl->epoch;
-            unsigned int spins = 0;
-            while (*rd != ep) {
-                if (++spins > P.ready_limit) {
-                    err |= CSM_ERRBIT_TIMEOUT;
-                    slot = 0xFFFFFFFEu;
-                    break;
-                }
-                __nanosleep(64);
-            }
-            __threadfence();
-        }
+        __threadfence();
     }
-    slot = __shfl_sync(0xffffffffu, slot, 0);
-    if (slot >= 0xFFFFFFFEu) return 0;
-    volatile const WorkItem *it = P.queue + slot;
+    pos = __shfl_sync(0xffffffffu, pos, 0);
+    if (pos == 0xFFFFFFFFu) return 0;
+    volatile const WorkItem *it = P.queue + (pos & P.qmask);
     if (lane == 0) {
         S.item_plan = it->plan;
         S.item_depth = it->depth;
@@ -468,17 +521,33 @@ __device__ int claim_item(WarpState &S, const EnumParams &P, unsigned int &err) 
     }
     if (lane < CSM_MAXQV) S.f[lane] = it->f[lane];
     __syncwarp();
-    if (S.item_depth == 0xFFFFFFFFu) return -1;  // null slot
-    return 1;
+    if (lane == 0) {
+        __threadfence();
+        atomicExch(P.seq + (pos & P.qmask), slot_stamp(ep, pos + P.qmask + 1));
+    }
+    __syncwarp();
+    return item_ok(S, P, CSM_BAD_ITEM, pos) ? 1 : 0;
 }
 
-__device__ bool take_ticket(WarpState &S, const EnumParams &P) {
+// Withdraws one outstanding work request (an idle warp that leaves without work).
+__device__ void withdraw_request(const EnumParams &P) {
+    unsigned int h = *(volatile unsigned int *)&P.ctrl->hungry;
+    for (int tries = 0; tries < 64 && h > 0; tries++) {
+        const unsigned int prev = atomicCAS(&P.ctrl->hungry, h, h - 1);
+        if (prev == h) return;
+        h = prev;
+    }
+}
+
+// Takes the next seed chunk or frontier item into S: 1 = taken, 0 = none left, -1 = a frontier
+// item that failed its check (skipped).
+__device__ int take_ticket(WarpState &S, const EnumParams &P) {
     const uint32_t lane = lane_id();
     unsigned long long t = 0;
     if (lane == 0) t = atomicAdd(&P.ctrl->ticket, 1ull);
     t = __shfl_sync(0xffffffffu, t, 0);
     const unsigned long long nt = *(volatile unsigned long long *)&P.ctrl->nticket;
-    if (t >= nt) return false;
+    if (t >= nt) return 0;
     if (P.frontier != nullptr) {
         const WorkItem *it = P.frontier + t;
         if (lane == 0) {
@@ -488,6 +557,8 @@ __device__ bool take_ticket(WarpState &S, const EnumParams &P) {
             S.item_hi = it->hi;
         }
         if (lane < CSM_MAXQV) S.f[lane] = it->f[lane];
+        __syncwarp();
+        if (!item_ok(S, P, CSM_BAD_FRONTIER, (uint32_t)t)) return -1;
     } else {
         // Seed chunk t: plan p with ticket_prefix[p] <= t < ticket_prefix[p+1].
         uint32_t lo = 0, hi = P.nplans;
@@ -508,7 +579,7 @@ __device__ bool take_ticket(WarpState &S, const EnumParams &P) {
         }
     }
     __syncwarp();
-    return true;
+    return 1;
 }
 
 __device__ void write_row(const EnumParams &P, const DevPlan *pl, const WarpState &S, uint32_t d, uint32_t w,
@@ -545,7 +616,7 @@ __device__ bool count_last_packed(WarpState &S, const EnumParams &P, const DevPl
             sib_b = b;
             continue;
         }
-        const uint2 ms = __ldg(P.g.meta + (size_t)__ldg(&lv->bn_rel[b]) * P.g.V + S.f[dep]);
+        const uint2 ms = list_of(P, __ldg(&lv->bn_rel[b]), S.f[dep], 400 + L);
         if (lane == 0) {
             S.poff[bb + b] = ms.x;  // level L's own slots: it is counted, never entered
             S.psz[bb + b] = ms.y;
@@ -561,7 +632,7 @@ __device__ bool count_last_packed(WarpState &S, const EnumParams &P, const DevPl
     if (lane < k) {
         sv = S.buf[d][ps + lane];
         if (sib_b != 0xFFu) {
-            const uint2 ms = __ldg(P.g.meta + (size_t)__ldg(&lv->bn_rel[sib_b]) * P.g.V + sv);
+            const uint2 ms = list_of(P, __ldg(&lv->bn_rel[sib_b]), sv, 500 + L);
             s_off = ms.x;
             s_sz = ms.y;
         }
@@ -603,6 +674,10 @@ __device__ bool count_last_packed(WarpState &S, const EnumParams &P, const DevPl
             w = e >> 1;
             scans++;
             ok = !(((oldm >> c_pv) & 1u) && (e & 1u)) && w != c_sv;
+            if (w >= P.g.V) {
+                record_bad(P, CSM_BAD_ENTRY, e, c_poff + (g - excl_j), 600 + L);
+                ok = false;
+            }
         }
         for (uint32_t t = 0; ok && t < d; t++) ok = S.f[t] != w;
         const uint32_t nlf_word = ok ? __ldg(nlf + (w >> 5)) : 0u;
@@ -623,9 +698,12 @@ __device__ bool count_last_packed(WarpState &S, const EnumParams &P, const DevPl
     return true;
 }
 
-// Runs one work item to completion.  Returns the number of matches counted.
+// Runs one work item to completion (or until the device clock passes `deadline`, when that is
+// nonzero: the rest of the item is then dropped and CSM_ERRBIT_TIMEOUT set).  Returns the number
+// of matches counted.
 __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, uint32_t &scans,
-                                       uint32_t &probes, uint32_t &tails, unsigned int &err) {
+                                       uint32_t &probes, uint32_t &tails, unsigned int &err,
+                                       unsigned long long deadline) {
     const uint32_t lane = lane_id();
     const DevPlan *pl = P.plans + S.item_plan;
     const uint32_t n = pl->n;
@@ -671,7 +749,16 @@ __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, uint32
     const uint32_t *nlf1 = bitmap(P, pl->nlf1);
 
     while (true) {
-        if (P.donate && ((++iter & 7u) == 0)) {
+        ++iter;
+        if (deadline && (iter & 63u) == 0) {
+            unsigned int late = 0;
+            if (lane == 0) late = device_ns() > deadline;
+            if (__shfl_sync(0xffffffffu, late, 0)) {
+                err |= CSM_ERRBIT_TIMEOUT;
+                break;
+            }
+        }
+        if (P.donate && (iter & 7u) == 0) {
             // Each idle warp posts one request; a busy warp that takes a request splits off
             // one piece of its pending work (and hands the request back if it has none).
             unsigned int granted = 0;
@@ -734,6 +821,10 @@ __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, uint32
                 cand = e >> 1;
                 scans++;
                 ok = !(((oldm >> piv) & 1u) && (e & 1u));
+                if (cand >= P.g.V) {
+                    record_bad(P, CSM_BAD_ENTRY, e, S.base[d] + idx, d);
+                    ok = false;
+                }
             }
             for (uint32_t k = 0; ok && k < d; k++) ok = S.f[k] != cand;
             // The NLF word is loaded now and tested after the probes, so its latency overlaps
@@ -919,22 +1010,32 @@ __global__ void __launch_bounds__(256, MINB) k_enumerate(EnumParams P) {
     // lane flushes them to the launch totals before they could wrap.
     uint32_t scans = 0, probes = 0, tails = 0;
     unsigned int err = 0;
+    const unsigned long long deadline = P.time_limit_ns ? P.ctrl->t_start + P.time_limit_ns : 0ull;
     bool have_source = true;  // seed tickets / frontier not yet exhausted
     // A warp counts as active from its start: blocks that become resident late (the GPU shared
     // with other kernels, or more blocks than fit) join the count when they start, so warps
     // that ran out of work never wait for blocks that have not started.
     if (lane == 0) atomicAdd(&P.ctrl->active, 1u);
     __syncwarp();
-    while (true) {
+    while (!(err & CSM_ERRBIT_TIMEOUT)) {
+        if (deadline) {
+            unsigned int late = 0;
+            if (lane == 0) late = device_ns() > deadline;
+            if (__shfl_sync(0xffffffffu, late, 0)) {
+                err |= CSM_ERRBIT_TIMEOUT;
+                break;
+            }
+        }
         int got = 0;
         if (have_source) {
-            got = take_ticket(S, P) ? 1 : 0;
+            got = take_ticket(S, P);
+            if (got < 0) continue;  // a frontier item that failed its check
             if (!got) have_source = false;
         }
-        if (!got) got = claim_item(S, P, err);
-        if (got < 0) continue;  // null slot
+        if (!got) got = claim_item(S, P);
         if (!got) {
-            // Become idle: wait (bounded) for donated work, leave when nobody holds work.
+            // Become idle: post one work request and wait (bounded) for donated work; leave
+            // when no warp holds work and the ring is empty, withdrawing the request.
             if (lane == 0) {
                 atomicSub(&P.ctrl->active, 1u);
                 atomicAdd(&P.ctrl->hungry, 1u);
@@ -942,30 +1043,33 @@ __global__ void __launch_bounds__(256, MINB) k_enumerate(EnumParams P) {
             __syncwarp();
             bool resumed = false;
             for (uint32_t it = 0; it < P.idle_limit; it++) {
-                const int c = claim_item(S, P, err);
-                if (c < 0) continue;  // null slot
-                if (c > 0) {
+                if (claim_item(S, P)) {
                     if (lane == 0) atomicAdd(&P.ctrl->active, 1u);
                     __syncwarp();
                     resumed = true;
                     break;
                 }
-                unsigned int act = 0, qr = 0, qw = 0;
+                unsigned int act = 0, qt = 0, qh = 0, late = 0;
                 if (lane == 0) {
                     act = *(volatile unsigned int *)&P.ctrl->active;
-                    qr = *(volatile unsigned int *)&P.ctrl->q_read;
-                    qw = *(volatile unsigned int *)&P.ctrl->q_write;
+                    qt = *(volatile unsigned int *)&P.ctrl->q_tail;
+                    qh = *(volatile unsigned int *)&P.ctrl->q_head;
+                    late = deadline && device_ns() > deadline;
                 }
                 act = __shfl_sync(0xffffffffu, act, 0);
-                qr = __shfl_sync(0xffffffffu, qr, 0);
-                qw = __shfl_sync(0xffffffffu, qw, 0);
-                if (qw > P.qcap) qw = P.qcap;
-                if (act == 0 && qr >= qw) break;
+                qt = __shfl_sync(0xffffffffu, qt, 0);
+                qh = __shfl_sync(0xffffffffu, qh, 0);
+                if (__shfl_sync(0xffffffffu, late, 0)) err |= CSM_ERRBIT_TIMEOUT;
+                if ((act == 0 && qt >= qh) || (err & CSM_ERRBIT_TIMEOUT)) break;
                 __nanosleep(512);
             }
-            if (!resumed) break;
+            if (!resumed) {
+                if (lane == 0) withdraw_request(P);
+                __syncwarp();
+                break;
+            }
         }
-        const unsigned long long c = run_item(S, P, scans, probes, tails, err);
+        const unsigned long long c = run_item(S, P, scans, probes, tails, err, deadline);
         if (lane == 0 && c) atomicAdd(P.counts + S.item_plan, c);
         if ((scans | probes | tails) >= (1u << 30)) {
             atomicAdd(&P.ctrl->scan_entries, (unsigned long long)scans);
@@ -1052,6 +1156,7 @@ __global__ void k_ctrl_reset(EnumControl *ctrl, uint32_t active, unsigned long l
     c.active = active;
     c.epoch = epoch;
     c.nticket = nticket;
+    c.t_start = device_ns();
     *ctrl = c;
 }
 
@@ -1072,8 +1177,7 @@ __global__ void k_expand_bound(EnumParams P, const WorkItem *items, const unsign
         const DevLevel *lv = &pl->lv[d];
         uint32_t sz = 0xFFFFFFFFu;
         if (lane < lv->nbn) {
-            const uint2 ms = P.g.meta[(size_t)lv->bn_rel[lane] * P.g.V + it->f[lv->bn_depth[lane]]];
-            sz = ms.y;
+            sz = list_of(P, lv->bn_rel[lane], it->f[lv->bn_depth[lane]], 800 + d).y;
         }
         for (int o = 16; o > 0; o >>= 1) sz = min(sz, __shfl_xor_sync(0xffffffffu, sz, o));
         if (lane == 0) acc += sz;

@@ -35,6 +35,7 @@ struct GraphView {
     const uint32_t *pool;    // adjacency entries
     uint32_t V;
     uint32_t R;
+    unsigned long long pool_cap;  // entries in `pool`
 };
 
 // First index in the sorted entry list whose neighbour id is >= w (entries are (id<<1)|flag).
@@ -92,9 +93,9 @@ struct EnumParams {
     const uint32_t *ticket_prefix;   // per plan: prefix of seed chunks (nplans + 1)
     const WorkItem *frontier;        // alternative work source (semi-BFS frontier)
     uint32_t nfrontier;
-    WorkItem *queue;                 // donation queue
-    uint32_t *ready;
-    uint32_t qcap;
+    WorkItem *queue;                 // donation ring (qmask + 1 slots)
+    unsigned long long *seq;         // per slot: epoch << 32 | position (see EnumControl)
+    uint32_t qmask;
     EnumControl *ctrl;
     unsigned long long *counts;      // per plan
     uint32_t mode;                   // 0 count, 1 materialize, 2 expand one level
@@ -105,7 +106,7 @@ struct EnumParams {
     uint32_t donate;
     uint32_t steal_min;
     uint32_t idle_limit;             // polls of an idle warp waiting for donated work
-    uint32_t ready_limit;            // polls of a claimed slot whose item is being written
+    unsigned long long time_limit_ns;  // >0: warps stop once the launch has run this long
     const unsigned int *abort_flag;  // nonzero: the batch update failed, skip enumeration
     const uint32_t *touched;         // bit per vertex: some batch key has it as list owner
 };

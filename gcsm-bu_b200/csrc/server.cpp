@@ -33,7 +33,7 @@ uint64_t now_ns() {
         .count();
 }
 
-constexpr uint32_t kSlotQueueItems = 1u << 21;
+constexpr uint32_t kSlotQueueItems = 1u << 18;  // donation ring slots per slot (reused)
 constexpr uint32_t kSlotMaxPlans = 4096;
 
 // The device range behind the frontier arena (bookkeeping in RangeAllocator).
@@ -121,8 +121,8 @@ class Server {
             if (e == cudaSuccess) e = cudaMalloc(&sl.sc.ctrl, sizeof(EnumControl));
             if (e == cudaSuccess) e = cudaMemset(sl.sc.ctrl, 0, sizeof(EnumControl));
             if (e == cudaSuccess) e = cudaMalloc(&sl.sc.queue, sizeof(WorkItem) * kSlotQueueItems);
-            if (e == cudaSuccess) e = cudaMalloc(&sl.sc.ready, sizeof(uint32_t) * kSlotQueueItems);
-            if (e == cudaSuccess) e = cudaMemset(sl.sc.ready, 0, sizeof(uint32_t) * kSlotQueueItems);
+            if (e == cudaSuccess) e = cudaMalloc(&sl.sc.seq, sizeof(unsigned long long) * kSlotQueueItems);
+            if (e == cudaSuccess) e = cudaMemset(sl.sc.seq, 0, sizeof(unsigned long long) * kSlotQueueItems);
             if (e == cudaSuccess) e = cudaMalloc(&sl.sc.seed_lo, sizeof(uint32_t) * 3 * kSlotMaxPlans);
             if (e == cudaSuccess) e = cudaMalloc(&sl.sc.ticket_prefix, sizeof(uint32_t) * (kSlotMaxPlans + 1));
             if (e != cudaSuccess) return cuda_fail(e, "slot scratch");
@@ -226,7 +226,7 @@ class Server {
             if (sl.stream) cudaStreamSynchronize(sl.stream);
             cudaFree(sl.sc.ctrl);
             cudaFree(sl.sc.queue);
-            cudaFree(sl.sc.ready);
+            cudaFree(sl.sc.seq);
             cudaFree(sl.sc.seed_lo);
             cudaFree(sl.sc.ticket_prefix);
             if (sl.pinned) cudaFreeHost(sl.pinned);

@@ -362,13 +362,17 @@ __global__ void k_scatter(uint32_t mu, const unsigned long long *ukeys, KeyLayou
     }
 }
 
-// Compaction: capacities recomputed from sizes, then every list copied to its new place.
-__global__ void k_recap(size_t n, const uint2 *meta, uint32_t *cap, unsigned long long *cap64) {
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        const uint32_t c = slack_capacity(meta[i].y);
-        cap[i] = c;
-        cap64[i] = c;
-    }
+// Compaction: the fresh-slack capacity of every list (from its size), as 64-bit values to be
+// prefix-summed into the new layout's offsets.  Nothing of the current layout changes.
+__global__ void k_fresh_caps(size_t n, const uint2 *meta, unsigned long long *cap64) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        cap64[i] = slack_capacity(meta[i].y);
+}
+
+// Compaction commit: capacities of the new layout.
+__global__ void k_set_caps(size_t n, const uint2 *meta, uint32_t *cap) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        cap[i] = slack_capacity(meta[i].y);
 }
 
 __global__ void k_copy_lists(size_t n, const uint2 *meta, const unsigned long long *newoff, const uint32_t *src,
@@ -424,12 +428,16 @@ __global__ void k_rel_delta(uint32_t m, const unsigned long long *keys, KeyLayou
 
 // Bit per vertex that owns a list some batch key belongs to (the key's source).  Keys are
 // sorted, so neighbouring lanes mostly share a word; one lane per distinct source sets it.
-__global__ void k_touched(uint32_t m, const unsigned long long *keys, KeyLayout kl, uint32_t *bits) {
+// Updates that match no relation carry CSM_INVALID_KEY (sorted to the end): they own no list,
+// and their all-ones source field is no vertex, so they are skipped.
+__global__ void k_touched(uint32_t m, const unsigned long long *keys, KeyLayout kl, uint32_t *bits, uint32_t words) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= m) return;
-    const uint32_t x = kl.src(keys[i]);
+    const unsigned long long k = keys[i];
+    if (k == CSM_INVALID_KEY) return;
+    const uint32_t x = kl.src(k);
     if (i > 0 && kl.src(keys[i - 1]) == x) return;
-    atomicOr(bits + (x >> 5), 1u << (x & 31));
+    if ((x >> 5) < words) atomicOr(bits + (x >> 5), 1u << (x & 31));
 }
 
 // Entry count of every relation (sum of its list sizes).  The loop is warp-uniform so that all
@@ -516,7 +524,7 @@ void store_rel_delta(uint32_t m, const unsigned long long *keys, KeyLayout kl, c
 void store_touched(uint32_t m, const unsigned long long *keys, KeyLayout kl, uint32_t *bits, uint32_t words,
                    cudaStream_t s) {
     cudaMemsetAsync(bits, 0, sizeof(uint32_t) * words, s);
-    if (m) k_touched<<<(m + 255) / 256, 256, 0, s>>>(m, keys, kl, bits);
+    if (m) k_touched<<<(m + 255) / 256, 256, 0, s>>>(m, keys, kl, bits, words);
 }
 
 void store_rel_sizes(const DeviceGraph &g, unsigned long long *out, cudaStream_t s) {
@@ -588,39 +596,43 @@ done:
 #undef CSM_TRY
 }
 
-// Re-lays every list out with fresh slack into `new_pool` (capacity new_cap entries).
-cudaError_t store_compact(DeviceGraph &g, uint32_t *new_pool, unsigned long long new_cap, cudaStream_t s,
-                          unsigned long long &used) {
+// Layout of a compaction, without changing the graph: `offsets` (nmeta + 1 entries, allocated
+// here; release with cudaFree) receives every list's offset in a fresh-slack layout, and `total`
+// the entries that layout needs.
+cudaError_t store_layout(const DeviceGraph &g, unsigned long long **offsets, unsigned long long &total, cudaStream_t s) {
     const size_t nmeta = (size_t)g.R * g.V;
     unsigned long long *cap64 = nullptr;
     void *temp = nullptr;
     size_t temp_bytes = 0;
+    *offsets = nullptr;
     cudaError_t e = cudaMalloc(&cap64, sizeof(unsigned long long) * (nmeta + 1));
     if (e != cudaSuccess) return e;
-    k_recap<<<grid_for(nmeta, 256), 256, 0, s>>>(nmeta, g.meta, g.cap, cap64);
-    cudaMemsetAsync(cap64 + nmeta, 0, sizeof(unsigned long long), s);
-    cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, cap64, cap64, nmeta + 1, s);
-    e = cudaMalloc(&temp, temp_bytes + 16);
+    k_fresh_caps<<<grid_for(nmeta, 256), 256, 0, s>>>(nmeta, g.meta, cap64);
+    if ((e = cudaMemsetAsync(cap64 + nmeta, 0, sizeof(unsigned long long), s)) == cudaSuccess &&
+        (e = cub::DeviceScan::ExclusiveSum(nullptr, temp_bytes, cap64, cap64, nmeta + 1, s)) == cudaSuccess &&
+        (e = cudaMalloc(&temp, temp_bytes + 16)) == cudaSuccess &&
+        (e = cub::DeviceScan::ExclusiveSum(temp, temp_bytes, cap64, cap64, nmeta + 1, s)) == cudaSuccess &&
+        (e = cudaMemcpyAsync(&total, cap64 + nmeta, sizeof(total), cudaMemcpyDeviceToHost, s)) == cudaSuccess)
+        e = cudaStreamSynchronize(s);
+    cudaFree(temp);
     if (e != cudaSuccess) {
         cudaFree(cap64);
         return e;
     }
-    cub::DeviceScan::ExclusiveSum(temp, temp_bytes, cap64, cap64, nmeta + 1, s);
-    unsigned long long total = 0;
-    cudaMemcpyAsync(&total, cap64 + nmeta, sizeof(total), cudaMemcpyDeviceToHost, s);
-    cudaStreamSynchronize(s);
-    if (total > new_cap) {
-        cudaFree(cap64);
-        cudaFree(temp);
-        return cudaErrorMemoryAllocation;
-    }
-    k_copy_lists<<<grid_for(nmeta * 32, 256), 256, 0, s>>>(nmeta, g.meta, cap64, g.pool, new_pool);
-    k_set_offsets<<<grid_for(nmeta, 256), 256, 0, s>>>(nmeta, cap64, g.meta);
-    cudaMemcpyAsync(g.pool_top, &total, sizeof(total), cudaMemcpyHostToDevice, s);
-    e = cudaStreamSynchronize(s);
-    used = total;
-    cudaFree(cap64);
-    cudaFree(temp);
+    *offsets = cap64;
+    return cudaGetLastError();
+}
+
+// Moves every list to `offsets` (from store_layout) inside `new_pool` and makes that layout the
+// graph's: offsets, capacities and the bump pointer.  The caller then swaps the pools.
+cudaError_t store_relayout(DeviceGraph &g, uint32_t *new_pool, const unsigned long long *offsets,
+                           unsigned long long total, cudaStream_t s) {
+    const size_t nmeta = (size_t)g.R * g.V;
+    k_copy_lists<<<grid_for(nmeta * 32, 256), 256, 0, s>>>(nmeta, g.meta, offsets, g.pool, new_pool);
+    k_set_offsets<<<grid_for(nmeta, 256), 256, 0, s>>>(nmeta, offsets, g.meta);
+    k_set_caps<<<grid_for(nmeta, 256), 256, 0, s>>>(nmeta, g.meta, g.cap);
+    cudaError_t e = cudaMemcpyAsync(g.pool_top, &total, sizeof(total), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     return e == cudaSuccess ? cudaGetLastError() : e;
 }
 

@@ -43,7 +43,7 @@ struct DeviceGraph {
     unsigned long long pool_cap = 0;
     unsigned long long *pool_top = nullptr;  // device bump pointer
     uint8_t *vlab = nullptr;               // [V] dense label or CSM_NO_LABEL
-    GraphView view() const { return GraphView{meta, pool, V, R}; }
+    GraphView view() const { return GraphView{meta, pool, V, R, pool_cap}; }
 };
 
 // Per-batch device scratch, sized for the largest batch.
@@ -88,7 +88,11 @@ void store_edge_stats(DeviceGraph &g, uint32_t rel, const uint32_t *bits_u, cons
                       unsigned long long *out, cudaStream_t s);
 cudaError_t store_build_from_keys(DeviceGraph &g, const unsigned long long *keys_sorted, uint32_t m, KeyLayout kl,
                                   cudaStream_t s, std::string &err);
-cudaError_t store_compact(DeviceGraph &g, uint32_t *new_pool, unsigned long long new_cap, cudaStream_t s,
-                          unsigned long long &used);
+// Compaction in two steps: store_layout computes a fresh-slack layout of the current lists
+// (offsets per list, allocated by the call, and the entries it needs) without changing the
+// graph; store_relayout moves the lists into a new pool along it and makes it current.
+cudaError_t store_layout(const DeviceGraph &g, unsigned long long **offsets, unsigned long long &total, cudaStream_t s);
+cudaError_t store_relayout(DeviceGraph &g, uint32_t *new_pool, const unsigned long long *offsets,
+                           unsigned long long total, cudaStream_t s);
 
 }  // namespace csm

@@ -82,6 +82,11 @@ typedef struct csm_config {
                                        planning (the reference plans once, before the stream) */
     int32_t semi_bfs_items_per_warp; /* dynamic semi-BFS (strategy 2) stops expanding once the
                                        frontier holds this many items per warp; 0 = 512 */
+    int32_t queue_slots;            /* work-donation ring of the enumeration: slots, a power of two
+                                       in [32, 2^24]; 0 = 2^18 (a full ring only costs balance) */
+    int32_t reserved0;
+    uint64_t time_limit_us;         /* >0: every enumeration launch stops after this many
+                                       microseconds; see csm_set_time_limit */
 } csm_config;
 
 /* Per-query result of one batch. */
@@ -116,7 +121,8 @@ typedef struct csm_stats {
     uint64_t tuned_occupancy;
     uint64_t graph_launches;        /* batches replayed from a CUDA graph */
     uint64_t replans;               /* re-plannings triggered by relation-size drift */
-    uint64_t reserved[2];
+    uint64_t donations_refused;     /* donations not made because the donation ring was full */
+    uint64_t reserved[1];
 } csm_stats;
 
 /* Fills `cfg` with the defaults (algorithm 0 with all switches on, as main.cpp). */
@@ -188,14 +194,19 @@ csm_status csm_apply_batch_device(csm_engine *engine, uint64_t n, const uint32_t
  * which every GPU that loads the library holds until the process exits.
  *  - Limits: at most CSM_STATIC_MAX_PLANS query edges over all registered queries, and no
  *    more updates than the batch capacity preallocated when the graph was loaded
- *    (csm_config.max_batch); larger requests fail with CSM_ERR_LIMIT.  The adjacency pool is
- *    never regrown: if a batch does not fit, the call fails with CSM_ERR_OOM (size
- *    csm_config.pool_entries for the stream).
- *  - The first call on a device looks up the array's device address; make that first call
+ *    (csm_config.max_batch); larger requests fail with CSM_ERR_LIMIT.  The work-donation ring
+ *    in the array has 65,536 slots (a full ring only costs balance, never a result).
+ *  - The adjacency pool is never compacted or regrown here.  A batch that could need more
+ *    room than is free (64 entries per update plus 2^20) is refused with CSM_ERR_LIMIT before
+ *    anything changes: apply a batch through csm_apply_batch_device (which compacts), or size
+ *    csm_config.pool_entries for the stream.  Should the pool still run out inside a batch,
+ *    the call fails with CSM_ERR_OOM and the engine refuses every later batch (recreate it).
+ *  - The first call of each engine looks up the array's device address; make that first call
  *    before any stream capture.
- *  - All calls on one device share the array, which keeps the last call's contents (the call
- *    clears what must start at zero).  Calls that overlap on the GPU — other streams, other
- *    engines, other threads — race on it: serialise them.
+ *  - All calls on one device share the array, which keeps the last call's contents; nothing
+ *    in it needs clearing (the control block is rewritten before every launch and the ring's
+ *    sequence words carry a launch epoch).  Calls that overlap on the GPU — other streams,
+ *    other engines, other threads — race on it: serialise them.
  */
 #define CSM_STATIC_SCRATCH_BYTES (8u << 20)
 #define CSM_STATIC_MAX_PLANS 4096u
@@ -203,6 +214,17 @@ csm_status csm_apply_batch_device_static(csm_engine *engine, uint64_t n, const u
                                          const uint32_t *d_dst, const uint32_t *d_elabel,
                                          const uint8_t *d_is_delete, void *stream,
                                          csm_batch_result *per_query_out);
+
+/*
+ * Bounds the enumeration time of later batches (no counterpart in the reference, whose
+ * kernels run to completion however long that takes).  Each enumeration launch of a batch
+ * stops once it has run `time_limit_us` microseconds (0 = no limit; the initial value is
+ * csm_config.time_limit_us).  A batch that hits the limit is still applied to the data graph in
+ * full — the update and index kernels do not depend on the counts — but its counts are
+ * incomplete: the call returns CSM_ERR_TIMEOUT with the partial counts in per_query_out, and
+ * the engine stays usable for the next batch.
+ */
+csm_status csm_set_time_limit(csm_engine *engine, uint64_t time_limit_us);
 
 /*
  * Per-query-edge split of the last batch's counts, in the query's qe_list_ order

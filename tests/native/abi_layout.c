@@ -15,6 +15,7 @@ int main(void) {
     F(csm_config, blocks_per_sm); F(csm_config, warps_per_block); F(csm_config, steal_chunk);
     F(csm_config, occupancy); F(csm_config, autotune_batches); F(csm_config, cuda_graphs);
     F(csm_config, replan_drift_pct); F(csm_config, semi_bfs_items_per_warp);
+    F(csm_config, queue_slots); F(csm_config, reserved0); F(csm_config, time_limit_us);
     F(csm_batch_result, positive); F(csm_batch_result, negative); F(csm_batch_result, inserted);
     F(csm_batch_result, deleted); F(csm_batch_result, latency_ns); F(csm_batch_result, apply_ns);
     F(csm_batch_result, enum_ns);
@@ -23,7 +24,7 @@ int main(void) {
     F(csm_stats, donations); F(csm_stats, enum_ns); F(csm_stats, apply_ns); F(csm_stats, pool_used);
     F(csm_stats, pool_capacity); F(csm_stats, compactions); F(csm_stats, tuned_strategy);
     F(csm_stats, tuned_steal_chunk); F(csm_stats, tuned_warps_per_block); F(csm_stats, tuned_occupancy);
-    F(csm_stats, graph_launches); F(csm_stats, replans);
+    F(csm_stats, graph_launches); F(csm_stats, replans); F(csm_stats, donations_refused);
     F(csm_server_config, device); F(csm_server_config, slots); F(csm_server_config, memory_budget);
     F(csm_server_config, min_frontier_bytes); F(csm_server_config, max_pending);
     F(csm_request_info, status); F(csm_request_info, nresults); F(csm_request_info, arrival_ns);

@@ -60,7 +60,7 @@ def test_create_fails_loudly_without_gpu():
 
 
 def test_struct_layouts():
-    assert ctypes.sizeof(csm.CsmConfig) == 4 * 8 + 8 * 4 + 4 * 8
+    assert ctypes.sizeof(csm.CsmConfig) == 4 * 8 + 8 * 4 + 4 * 8 + 4 * 2 + 8
     assert ctypes.sizeof(csm.CsmBatchResult) == 64
     assert ctypes.sizeof(csm.CsmStats) == 20 * 8
     assert ctypes.sizeof(csm.CsmServerConfig) == 4 + 4 + 8 + 8 + 4 + 7 * 4
