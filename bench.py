@@ -1,10 +1,13 @@
 """Benchmark of the batch-update incremental matching path.
 
-Workload (default): the Amazon-shaped configuration — Chung-Lu graph, 400k vertices, 2.4M
-edges, exponent 2.1, 6 Zipf(1.0) vertex labels; ten 6-vertex standing queries (5 dense, 5
-trees) sampled from the graph; 240k updates (90% insertions of held-out edges, 10% deletions)
-in batches of 65,536.  Seeded synthetic data stands in for the datasets the reference's
-experiments download.
+Workload (default, --config c3): the LiveJournal-shaped heavy-vertex configuration — Chung-Lu
+graph, 4.8M vertices, 43M edges (38.7M initial, 10% held out for insertions), exponent 1.9,
+20 Zipf(1.2) vertex labels; four dense 8-vertex standing queries; 4.3M updates (50% insertions
+of held-out edges, 50% deletions) in batches of 1,000,000.  The queries are sampled from the
+subgraph of the 12 rarest labels and kept when their estimated matches per batch are bounded
+(csm.gen, config c3).  --config c2 is the Amazon-shaped configuration (400k vertices, 2.4M
+edges, ten 6-vertex queries, 65,536-update batches).  Seeded synthetic data stands in for the
+datasets the reference's experiments download.
 
 A step applies one update batch and counts its incremental matches (positive and negative)
 for all standing queries.  The stream of four batches is followed by its inverse (each batch
@@ -41,7 +44,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=8)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2")
+    ap.add_argument("--config", default="c3")
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--nqueries", type=int, default=None)
     ap.add_argument("--batch", type=int, default=None, help="override the configuration's batch size")
@@ -223,7 +226,7 @@ def run_reference(args, w, world, rank):
         return
     threads = os.cpu_count() or 1
     plan = step_plan(w, args.warmup + args.steps)
-    budget = float(os.environ.get("CSM_REF_BUDGET_S", "150"))
+    budget = float(os.environ.get("CSM_REF_BUDGET_S", "90"))
     matches, t_total, items, lat = oracle_sample(w, plan, budget, warmup=args.warmup)
     value = matches / t_total if t_total else 0.0
     out = {
@@ -245,8 +248,12 @@ def workload_config(w, args, world):
     return {"workload": f"{w.name}: Chung-Lu {len(w.data.vlabels)} vertices, {len(w.data.src)} initial edges;"
                         f" step = one {w.batch_size}-update batch for one of {len(w.queries)} standing"
                         " queries (stream, then its inverse)",
-            "batch_size": w.batch_size, "queries": len(w.queries), "search_strategy": args.strategy,
-            "parallelism": f"replicas x{world}",
+            "batch_size": w.batch_size, "queries": len(w.queries),
+            "query_shapes": [f"{q.nv}v{len(q.src)}e" for q in w.queries],
+            "query_rule": (f"sampled from the subgraph of labels >= {w.meta['query_min_label']}, kept when the "
+                           f"estimated matches per batch <= {w.meta['query_bound']:.0e}")
+            if w.meta.get("query_bound") else "sampled from the data graph",
+            "search_strategy": args.strategy, "parallelism": f"replicas x{world}",
             "l2": "inputs larger than L2 (each engine's adjacency pool exceeds the 126 MB L2)"}
 
 
