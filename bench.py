@@ -50,6 +50,8 @@ def parse():
     ap.add_argument("--batch", type=int, default=None, help="override the configuration's batch size")
     ap.add_argument("--strategy", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cli-leg", action="store_true",
+                    help="skip csmg --algorithm 1 on the insertion stream (the files the reference arm runs)")
     ap.add_argument("--cpu-sample-queries", type=int, default=10)
     ap.add_argument("--form", default="plain", choices=["plain", "batched", "served"],
                     help="plain: one engine per standing query, a step is one batch for one query; "
@@ -218,29 +220,109 @@ def cpu_baseline(w, args, budget_s=20.0):
                       f"{matches} matches in {t:.1f} s"}
 
 
+REF_BUILD = os.path.join(ROOT, "oracle", "_ref", "csmg_ref")
+
+
+def insertion_stream_files(w, td):
+    """The reference's text files for the insertion half of the stream: data graph, the
+    stream's insertions in order (the reference reads no deletions, graph.cpp:507-551), one
+    query file per standing query.  Returns (data, updates, [queries], batch size)."""
+    from csm import Batch, textio
+    df, uf = os.path.join(td, "data.graph"), os.path.join(td, "updates.graph")
+    textio.write_data(df, w.data)
+    ins = []
+    for b in w.batches:
+        keep = b.is_delete == 0 if b.is_delete is not None else np.ones(len(b.src), dtype=bool)
+        ins.append(Batch(b.src[keep], b.dst[keep], b.elabels[keep]))
+    textio.write_updates(uf, ins)
+    qfs = []
+    for qi, q in enumerate(w.queries):
+        qfs.append(os.path.join(td, f"query{qi}.graph"))
+        textio.write_query(qfs[-1], q)
+    n_ins = sum(len(b.src) for b in ins)
+    return df, uf, qfs, max(1, (w.batch_size + 1) // 2), n_ins
+
+
+def run_cli(cmd, timeout_s):
+    """Runs a csmg-compatible tool; parses the reference's result lines
+    (technique_permutation.h:129-130, :224)."""
+    import re
+    t0 = time.perf_counter()
+    p = subprocess.run(["timeout", "-k", "30", str(int(timeout_s))] + cmd, capture_output=True, text=True)
+    m = re.search(r"^Incremental Matching, time \(ms\): (\d+)\(host\), (\d+)\(kernel\)", p.stdout, re.M)
+    c = re.search(r"^Num Positive Matches: (\d+)", p.stdout, re.M)
+    return {"rc": p.returncode, "host_ms": int(m.group(1)) if m else None, "kernel_ms": int(m.group(2)) if m else None,
+            "positive": int(c.group(1)) if c else None, "wall_s": round(time.perf_counter() - t0, 1)}
+
+
+def insertion_stream_runs(w, tool, timeout_s):
+    """`tool --algorithm 1` (the GCSM-BU preset) on the insertion stream, one process per standing
+    query as the reference's experiments run it (run_csm.py:153-161)."""
+    import tempfile
+    with tempfile.TemporaryDirectory() as td:
+        t0 = time.perf_counter()
+        df, uf, qfs, bsz, n_ins = insertion_stream_files(w, td)
+        log(f"insertion-stream files written ({time.perf_counter() - t0:.0f} s)")
+        rows = []
+        for qi, qf in enumerate(qfs):
+            r = run_cli([tool, "--query", qf, "--data", df, "--update", uf, "--batch_size", str(bsz),
+                         "--algorithm", "1"], timeout_s)
+            r["query"] = qi
+            rows.append(r)
+            log(f"{os.path.basename(tool)} query {qi}: {r}")
+    ok = [r for r in rows if r["rc"] == 0 and r["host_ms"] is not None and r["positive"] is not None]
+    host_ms = sum(r["host_ms"] for r in ok)
+    pos = sum(r["positive"] for r in ok)
+    return {"batches": f"{n_ins} insertions of the stream in batches of {bsz}", "nbatches": -(-n_ins // bsz),
+            "queries": rows,
+            "completed": len(ok) == len(rows), "host_ms_total": host_ms, "positive_total": pos,
+            "matches_per_s": pos / (host_ms / 1e3) if host_ms else None}
+
+
 def run_reference(args, w, world, rank):
-    """The CPU implementation of the path (the oracle port; the reference itself runs only on
-    a GPU) on all host threads, over the same (query, batch) steps as the GPU arm; each step is
-    a time-bounded sample of its work."""
+    """The reference's own implementation of the path: GCSM-BU is GPU-only (main.cpp has no CPU
+    path), so this arm runs the reference build (oracle/_ref/csmg_ref, compiled from the
+    reference's sources for sm_100a) on this GPU with its own preset (--algorithm 1), on the
+    insertion half of the bench stream (it reads no deletions), one process per query as its
+    experiments run.  Value = positive matches / its "Incremental Matching" time.  Without the
+    build (or a GPU) the CPU oracle port stands in, on time-bounded samples of the same steps."""
     if rank != 0:
         return
     threads = os.cpu_count() or 1
+    base = {"metric": "incremental matches/sec", "unit": "matches/s", "impl": "reference", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u32", "data": "synthetic", "config": workload_config(w, args, world)}
+    if os.path.exists(REF_BUILD) and os.environ.get("CSM_REF_ARM", "build") == "build" and gpu_present():
+        res = insertion_stream_runs(w, REF_BUILD, float(os.environ.get("CSM_REF_TIMEOUT_S", "900")))
+        if res["completed"] and res["matches_per_s"]:
+            value = res["matches_per_s"]
+            out = dict(base, value=value, ms_per_step=res["host_ms_total"] / max(1, res["nbatches"] * len(w.queries)))
+            out["cpu_baseline"] = {"value": value, "unit": "matches/s", "cores": 1, "kind": "reference",
+                                   "sample": "the reference GCSM-BU build (sm_100a, --algorithm 1) on this GPU, one "
+                                             "host thread: every query over " + res["batches"]}
+            out["reference_build"] = res
+            out["e2e"] = {"value": value, "unit": "matches/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+            print(json.dumps(out))
+            return
+        log("reference build did not complete; falling back to the CPU oracle port")
     plan = step_plan(w, args.warmup + args.steps)
     budget = float(os.environ.get("CSM_REF_BUDGET_S", "90"))
     matches, t_total, items, lat = oracle_sample(w, plan, budget, warmup=args.warmup)
     value = matches / t_total if t_total else 0.0
-    out = {
-        "metric": "incremental matches/sec", "value": value, "unit": "matches/s", "impl": "reference",
-        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t_total / args.steps,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-        "config": workload_config(w, args, world),
-        "cpu_baseline": {"value": value, "unit": "matches/s", "cores": threads, "kind": "port",
-                         "sample": f"{args.steps} (query, batch) steps, each batch applied in full with counting "
-                                   f"capped at {budget / args.steps:.1f} s per step: {items} seed items, "
-                                   f"{matches} matches"},
-        "e2e": {"value": value, "unit": "matches/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
+    out = dict(base, value=value, ms_per_step=1e3 * t_total / args.steps)
+    out["cpu_baseline"] = {"value": value, "unit": "matches/s", "cores": threads, "kind": "port",
+                           "sample": f"{args.steps} (query, batch) steps, each batch applied in full with counting "
+                                     f"capped at {budget / args.steps:.1f} s per step: {items} seed items, "
+                                     f"{matches} matches"}
+    out["e2e"] = {"value": value, "unit": "matches/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     print(json.dumps(out))
+
+
+def gpu_present():
+    try:
+        return subprocess.run(["nvidia-smi", "-L"], capture_output=True, text=True, timeout=30).returncode == 0
+    except (OSError, subprocess.TimeoutExpired):
+        return False
 
 
 def workload_config(w, args, world):
@@ -411,6 +493,10 @@ def run_ours(args, w, world, rank, local):
     }
     if world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(w, args)
+    if world == 1 and not args.no_cli_leg:
+        # This engine's csmg on the files the reference arm runs the reference build on.
+        import csm
+        out["insertion_stream_csmg"] = insertion_stream_runs(w, csm.CSMG_PATH, 900)
     print(json.dumps(out))
 
 

@@ -14,12 +14,26 @@ import numpy as np
 from . import Batch, DataGraph, QueryGraph
 
 
+def _write_rows(f, tag: str, *cols) -> None:
+    """Lines `tag c0 c1 ...` of integer columns (pandas' C writer for large arrays)."""
+    n = len(cols[0])
+    if n == 0:
+        return
+    if n < 100_000:
+        f.write("".join(tag + " " + " ".join(str(int(c[i])) for c in cols) + "\n" for i in range(n)))
+        return
+    import pandas as pd
+    df = pd.DataFrame({"t": np.full(n, tag, dtype=object), **{str(k): np.asarray(c, dtype=np.int64)
+                                                              for k, c in enumerate(cols)}})
+    df.to_csv(f, sep=" ", header=False, index=False, lineterminator="\n")
+
+
 def write_graph(path: str, vlabels, src, dst, elabels, header: str = "t # 0") -> None:
     vlabels = np.asarray(vlabels)
     with open(path, "w") as f:
         f.write(header + "\n")
-        f.write("".join(f"v {i} {int(l)}\n" for i, l in enumerate(vlabels)))
-        f.write("".join(f"e {int(a)} {int(b)} {int(l)}\n" for a, b, l in zip(src, dst, elabels)))
+        _write_rows(f, "v", np.arange(len(vlabels)), vlabels)
+        _write_rows(f, "e", src, dst, elabels)
 
 
 def write_query(path: str, q: QueryGraph) -> None:
@@ -34,6 +48,9 @@ def write_updates(path: str, batches: Sequence[Batch]) -> None:
     with open(path, "w") as f:
         for b in batches:
             dl = b.is_delete if b.is_delete is not None else np.zeros(len(b.src), dtype=np.uint8)
+            if not np.any(dl):
+                _write_rows(f, "e", b.src, b.dst, b.elabels)
+                continue
             f.write("".join(f"{'-e' if d else 'e'} {int(x)} {int(y)} {int(l)}\n"
                             for x, y, l, d in zip(b.src, b.dst, b.elabels, dl)))
 
