@@ -45,9 +45,18 @@ struct DevLevel {
     uint16_t old_mask;            // bit k: backward edge k must not be a batch edge
     uint8_t qv;                   // query vertex id
     uint8_t bn_base;              // first slot of this level's lists in a flat per-plan array
-    uint32_t nlf_bitmap;          // candidate bitmap (NLF filter) of this query vertex
-    uint32_t pad1[2];
+    // Candidate bitmap (NLF filter) of this query vertex, or CSM_NO_BITMAP when every query
+    // neighbour of the vertex is a backward neighbour: a candidate adjacent to all of them
+    // already has the neighbour counts the filter asks for.
+    uint32_t nlf_bitmap;
+    // Bit j: the query vertex at depth j < this level has this level's label.  Lists are
+    // label-partitioned, so a candidate can only coincide with those prefix vertices.
+    uint16_t excl_mask;
+    uint16_t pad0;
+    uint32_t pad1;
 };
+
+#define CSM_NO_BITMAP 0xFFFFFFFFu
 
 struct DevTailTerm {
     int64_t coef;

@@ -47,6 +47,7 @@ struct __align__(16) WarpState {
     uint8_t bnb[CSM_MAXQV];
     uint32_t nlf[CSM_MAXQV];
     uint16_t oldm[CSM_MAXQV];
+    uint16_t exm[CSM_MAXQV];   // per level: prefix depths the candidate may coincide with
     uint8_t nbuf[CSM_MAXQV];
     uint8_t pos[CSM_MAXQV];
     uint8_t piv[CSM_MAXQV];
@@ -270,6 +271,7 @@ __device__ void enter_level(WarpState &S, const EnumParams &P, const DevPlan *pl
         S.pos[d] = 0;
         S.oldm[d] = __ldg(&lv->old_mask);
         S.nlf[d] = __ldg(&lv->nlf_bitmap);
+        S.exm[d] = __ldg(&lv->excl_mask);
     }
     __syncwarp();
     if (d + 1 == pl->tail_start && pl->tail_start < pl->n && pl->tail.lane_par) prep_tail_shared(S, P, pl, d);
@@ -604,7 +606,9 @@ __device__ bool count_last_packed(WarpState &S, const EnumParams &P, const DevPl
     const DevLevel *lv = &pl->lv[L];
     const uint32_t nbn = __ldg(&lv->nbn);
     const uint32_t oldm = __ldg(&lv->old_mask);
-    const uint32_t *nlf = bitmap(P, __ldg(&lv->nlf_bitmap));
+    const uint32_t nlf_id = __ldg(&lv->nlf_bitmap);
+    const uint32_t *nlf = nlf_id == CSM_NO_BITMAP ? nullptr : bitmap(P, nlf_id);
+    const uint32_t exm = __ldg(&lv->excl_mask) & ((1u << d) - 1u);  // depth d is the sibling itself
     const uint32_t ps = S.pos[d], k = S.nbuf[d] - ps;
     // Shared lists: backward neighbours matched before depth d (same for every sibling).
     // sib_b = the backward neighbour at depth d (at most one), whose list is the sibling's own.
@@ -679,8 +683,8 @@ __device__ bool count_last_packed(WarpState &S, const EnumParams &P, const DevPl
                 ok = false;
             }
         }
-        for (uint32_t t = 0; ok && t < d; t++) ok = S.f[t] != w;
-        const uint32_t nlf_word = ok ? __ldg(nlf + (w >> 5)) : 0u;
+        for (uint32_t em = exm; ok && em; em &= em - 1) ok = S.f[__ffs(em) - 1] != w;
+        const uint32_t nlf_word = !ok ? 0u : (nlf ? __ldg(nlf + (w >> 5)) : 0xFFFFFFFFu);
         for (uint32_t b = 0; ok && b < nbn; b++) {
             if (b == c_pv) continue;
             const uint32_t *list = b == sib_b ? P.g.pool + c_soff : P.g.pool + S.poff[bb + b];
@@ -696,6 +700,128 @@ __device__ bool count_last_packed(WarpState &S, const EnumParams &P, const DevPl
     if (lane == 0) S.pos[d] = S.nbuf[d];
     __syncwarp();
     return true;
+}
+
+// Last level of a counting plan without a tail: the matches are the pivot-list candidates that
+// pass the flag rule, injectivity and membership in the one other backward list, i.e. a
+// filtered count of a sorted-list intersection (the shape of the last level of every dense plan
+// measured: two backward neighbours).  The other list's offset, size, cursor and flag rule stay
+// in registers for the whole scan instead of being re-read from the warp's shared state for
+// every 32 candidates.  Every 8 chunks the warp answers work requests (donating the upper half
+// of the remaining range) and checks the time limit.  Returns the count; the level is left
+// exhausted (S.lo[d] >= S.hi[d]).
+constexpr uint32_t kLastLists = 1;
+
+__device__ unsigned long long count_last_level(WarpState &S, const EnumParams &P, const DevPlan *pl, uint32_t L0,
+                                               uint32_t d, uint32_t &scans, uint32_t &probes, unsigned int &err,
+                                               unsigned long long deadline) {
+    const uint32_t lane = lane_id();
+    const uint32_t nbn = S.nbn[d], piv = S.piv[d], bb = S.bnb[d];
+    const uint32_t oldm = S.oldm[d], exm = S.exm[d], nlf_id = S.nlf[d];
+    const bool piv_old = (oldm >> piv) & 1u;
+    const uint32_t *nlf = nlf_id == CSM_NO_BITMAP ? nullptr : bitmap(P, nlf_id);
+    const uint32_t *base = P.g.pool + S.base[d];
+    uint32_t l_off[kLastLists], l_size[kLastLists], l_cur[kLastLists];
+    uint32_t l_old = 0;  // bit j: list j's batch entries do not count
+    uint32_t nl = 0;
+#pragma unroll
+    for (uint32_t j = 0; j < kLastLists; j++) l_off[j] = l_size[j] = l_cur[j] = 0;
+    for (uint32_t k = 0; k < nbn; k++) {
+        if (k == piv) continue;
+#pragma unroll
+        for (uint32_t j = 0; j < kLastLists; j++)
+            if (j == nl) {
+                l_off[j] = S.poff[bb + k];
+                l_size[j] = S.psz[bb + k];
+                l_old |= ((oldm >> k) & 1u) << j;
+            }
+        nl++;
+    }
+    uint32_t lo = S.lo[d], hi = S.hi[d];
+    unsigned long long cnt = 0;
+    for (uint32_t chunk = 1; lo < hi; lo += 32, chunk++) {
+        const uint32_t idx = lo + lane;
+        const bool in = idx < hi;
+        bool ok = in;
+        uint32_t cand = 0;
+        if (ok) {
+            const uint32_t e = __ldg(base + idx);
+            cand = e >> 1;
+            scans++;
+            ok = !(piv_old && (e & 1u));
+            if (cand >= P.g.V) {
+                record_bad(P, CSM_BAD_ENTRY, e, S.base[d] + idx, d);
+                ok = false;
+            }
+        }
+        for (uint32_t em = exm; ok && em; em &= em - 1) ok = S.f[__ffs(em) - 1] != cand;
+        const uint32_t nlf_word = !ok ? 0u : (nlf ? __ldg(nlf + (cand >> 5)) : 0xFFFFFFFFu);
+        const uint32_t vmask = __ballot_sync(0xffffffffu, in);
+        const uint32_t target = __shfl_sync(0xffffffffu, cand, 31 - __clz(vmask));
+        const uint32_t key_hi = (target + 1) << 1;
+        uint32_t win[kLastLists];
+#pragma unroll
+        for (uint32_t j = 0; j < kLastLists; j++)
+            win[j] = (j < nl && l_cur[j] + lane < l_size[j]) ? __ldg(P.g.pool + l_off[j] + l_cur[j] + lane) : 0xFFFFFFFFu;
+#pragma unroll
+        for (uint32_t j = 0; j < kLastLists; j++) {
+            if (j >= nl) break;
+            const uint32_t below = __ballot_sync(0xffffffffu, win[j] < key_hi);
+            uint32_t e = 0xFFFFFFFFu, nhi;
+            if (below != 0xffffffffu) {
+                nhi = l_cur[j] + __popc(below);
+                const uint32_t pos = shfl_lower_bound(win[j], cand << 1);
+                const uint32_t got = __shfl_sync(0xffffffffu, win[j], pos);
+                if ((got >> 1) == cand && got != 0xFFFFFFFFu) e = got;
+            } else {
+                const uint32_t *L = P.g.pool + l_off[j];
+                nhi = warp_lower_bound(L, l_cur[j] + 32, l_size[j], key_hi, lane);
+                if (ok) e = find_entry(L + l_cur[j], nhi - l_cur[j], cand);
+            }
+            if (ok) {
+                probes++;
+                ok = e != 0xFFFFFFFFu && !(((l_old >> j) & 1u) && (e & 1u));
+            }
+            l_cur[j] = nhi;
+        }
+        if (ok) ok = (nlf_word >> (cand & 31)) & 1u;
+        cnt += __popc(__ballot_sync(0xffffffffu, ok));
+        if ((chunk & 7u) == 0 && lo + 32 < hi) {
+            if (deadline) {
+                unsigned int late = 0;
+                if (lane == 0) late = device_ns() > deadline;
+                if (__shfl_sync(0xffffffffu, late, 0)) {
+                    err |= CSM_ERRBIT_TIMEOUT;
+                    break;
+                }
+            }
+            if (P.donate) {
+                unsigned int granted = 0;
+                if (lane == 0) {
+                    const unsigned int h = *(volatile unsigned int *)&P.ctrl->hungry;
+                    granted = h > 0 && atomicCAS(&P.ctrl->hungry, h, h - 1) == h;
+                }
+                if (__shfl_sync(0xffffffffu, granted, 0)) {
+                    // The remaining range [lo + 32, hi) is this level's pending work.
+                    if (lane == 0) {
+                        S.lo[d] = lo + 32;
+                        S.hi[d] = hi;
+                    }
+                    __syncwarp();
+                    if (!try_donate(S, P, pl, L0, d) && lane == 0) atomicAdd(&P.ctrl->hungry, 1u);
+                    hi = S.hi[d];
+                    __syncwarp();
+                }
+            }
+        }
+    }
+    __syncwarp();
+    if (lane == 0) {
+        S.lo[d] = hi;
+        S.hi[d] = hi;
+    }
+    __syncwarp();
+    return cnt;
 }
 
 // Runs one work item to completion (or until the device clock passes `deadline`, when that is
@@ -802,6 +928,11 @@ __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, uint32
             d--;
             continue;
         }
+        if (d + 1 == n && E == n && d >= 2 && P.mode == CSM_ENUM_MODE_COUNT && S.nbn[d] <= kLastLists + 1) {
+            cnt += count_last_level(S, P, pl, L0, d, scans, probes, err, deadline);
+            if (err & CSM_ERRBIT_TIMEOUT) break;
+            continue;
+        }
         // Scan the next 32 candidates of level d.
         const uint32_t idx = S.lo[d] + lane;
         bool ok = idx < S.hi[d];
@@ -826,10 +957,12 @@ __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, uint32
                     ok = false;
                 }
             }
-            for (uint32_t k = 0; ok && k < d; k++) ok = S.f[k] != cand;
+            for (uint32_t em = S.exm[d]; ok && em; em &= em - 1) ok = S.f[__ffs(em) - 1] != cand;
             // The NLF word is loaded now and tested after the probes, so its latency overlaps
             // theirs (probes are warp-wide and do not depend on it).
-            const uint32_t nlf_word = ok ? __ldg(bitmap(P, S.nlf[d]) + (cand >> 5)) : 0u;
+            const uint32_t nlf_id = S.nlf[d];
+            const uint32_t nlf_word =
+                !ok ? 0u : (nlf_id == CSM_NO_BITMAP ? 0xFFFFFFFFu : __ldg(bitmap(P, nlf_id) + (cand >> 5)));
             // Membership in the other backward lists.  The chunk's candidates ascend, so each
             // list keeps a cursor.  The 32 entries at the cursor are read first: when they
             // reach past the chunk's largest candidate, the window is in registers and

@@ -518,8 +518,11 @@ std::vector<HostPlan> build_plans(const Query &q, uint16_t query_id, uint32_t nl
             lv.bn_base = (uint8_t)bn_base;
             bn_base += (uint32_t)hp.bn[d].size();
             lv.qv = order[d];
-            lv.nlf_bitmap = nlf_base + order[d];
             lv.nbn = (uint8_t)hp.bn[d].size();
+            // All query neighbours matched before this level: the NLF filter is implied.
+            lv.nlf_bitmap = hp.bn[d].size() == q.nbrs[order[d]].size() ? CSM_NO_BITMAP : nlf_base + order[d];
+            for (uint32_t j = 0; j < d; j++)
+                if (q.vlabel[order[j]] == q.vlabel[order[d]]) lv.excl_mask |= (uint16_t)(1u << j);
             for (size_t k = 0; k < hp.bn[d].size(); k++) {
                 uint32_t bu = order[hp.bn[d][k]];
                 lv.bn_depth[k] = hp.bn[d][k];

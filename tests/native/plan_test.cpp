@@ -117,6 +117,16 @@ int main() {
                     if (d == 1) want.erase(0), got.erase(0);  // the seed edge itself
                     if (want != got) return fail("backward neighbours", qn, (int)pi);
                     if (want.empty() && d > 1) return fail("disconnected prefix", qn, (int)pi);
+                    if (d < 2) continue;
+                    // Injectivity is checked against the same-label prefix depths only, and the
+                    // NLF filter is dropped exactly where every query neighbour is backward.
+                    const DevLevel &lv = hp.dev.lv[d];
+                    for (uint32_t j = 0; j < n; j++) {
+                        const bool same = j < d && q.vlabel[hp.order[j]] == q.vlabel[hp.order[d]];
+                        if (same != (((lv.excl_mask >> j) & 1u) != 0)) return fail("level exclusion depths", qn, (int)pi);
+                    }
+                    const bool all_back = hp.bn[d].size() == q.nbrs[hp.order[d]].size();
+                    if (all_back != (lv.nlf_bitmap == CSM_NO_BITMAP)) return fail("implied NLF filter", qn, (int)pi);
                 }
                 const int ts = hp.tail_start;
                 for (uint32_t d = (uint32_t)ts; d < n; d++) {
