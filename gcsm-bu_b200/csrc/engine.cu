@@ -533,6 +533,11 @@ csm_status Engine::install_plans(const std::vector<EdgeStats> &stats) {
     CSM_CUDA(cudaStreamSynchronize(stream_));
     plans_ = std::move(plans);
     plan_begin_ = std::move(begin);
+    // The kernel variant with the last-level intersection loop pays only where a plan ends
+    // without a Cartesian tail (a last level the loop can count).
+    last_loop_ = false;
+    for (const auto &hp : plans_)
+        if (hp.dev.tail_start == hp.dev.n && hp.dev.n >= 3) last_loop_ = true;
     return CSM_OK;
 }
 
@@ -1106,6 +1111,7 @@ csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
     P.time_limit_ns = time_limit_us_ * 1000ull;
     P.abort_flag = phase == CSM_PHASE_INS ? bs_.error : nullptr;
     P.touched = d_touched_;
+    P.last_loop = last_loop_ ? 1u : 0u;
     P.rows = d_rows_;
     P.row_cap = row_cap_;
     const bool rows = cfg_.materialize_rows > 0;

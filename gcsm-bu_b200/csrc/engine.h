@@ -187,6 +187,7 @@ class Engine {
     uint32_t qcap_ = 0;
     uint64_t time_limit_us_ = 0;              // per enumeration launch; 0 = none
     csm_status deferred_ = CSM_OK;            // timeout / overflow of this batch, reported at its end
+    bool last_loop_ = false;                  // launch the kernel variant with the last-level loop
     unsigned long long last_frontier_rows_ = 0;
     // CUDA graphs of whole batches (depth-first strategies), keyed by what the capture bakes in.
     struct GraphKey {

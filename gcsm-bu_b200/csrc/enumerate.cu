@@ -827,6 +827,7 @@ __device__ unsigned long long count_last_level(WarpState &S, const EnumParams &P
 // Runs one work item to completion (or until the device clock passes `deadline`, when that is
 // nonzero: the rest of the item is then dropped and CSM_ERRBIT_TIMEOUT set).  Returns the number
 // of matches counted.
+template <bool LASTLOOP>
 __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, uint32_t &scans,
                                        uint32_t &probes, uint32_t &tails, unsigned int &err,
                                        unsigned long long deadline) {
@@ -928,7 +929,7 @@ __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, uint32
             d--;
             continue;
         }
-        if (d + 1 == n && E == n && d >= 2 && P.mode == CSM_ENUM_MODE_COUNT && S.nbn[d] <= kLastLists + 1) {
+        if (LASTLOOP && d + 1 == n && E == n && d >= 2 && P.mode == CSM_ENUM_MODE_COUNT && S.nbn[d] <= kLastLists + 1) {
             cnt += count_last_level(S, P, pl, L0, d, scans, probes, err, deadline);
             if (err & CSM_ERRBIT_TIMEOUT) break;
             continue;
@@ -1133,7 +1134,7 @@ __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, uint32
 }
 
 // MINB resident blocks of 256 threads per SM: the register budget per thread follows from it.
-template <int MINB>
+template <int MINB, bool LASTLOOP>
 __global__ void __launch_bounds__(256, MINB) k_enumerate(EnumParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
     WarpState &S = reinterpret_cast<WarpState *>(smem)[threadIdx.x >> 5];
@@ -1202,7 +1203,7 @@ __global__ void __launch_bounds__(256, MINB) k_enumerate(EnumParams P) {
                 break;
             }
         }
-        const unsigned long long c = run_item(S, P, scans, probes, tails, err, deadline);
+        const unsigned long long c = run_item<LASTLOOP>(S, P, scans, probes, tails, err, deadline);
         if (lane == 0 && c) atomicAdd(P.counts + S.item_plan, c);
         if ((scans | probes | tails) >= (1u << 30)) {
             atomicAdd(&P.ctrl->scan_entries, (unsigned long long)scans);
@@ -1324,28 +1325,32 @@ size_t enum_smem_bytes(int warps_per_block) { return sizeof(WarpState) * (size_t
 
 namespace {
 using EnumKernel = void (*)(EnumParams);
-EnumKernel enum_kernel(int occupancy) {
+EnumKernel enum_kernel(int occupancy, bool last_loop) {
     switch (occupancy) {
-        case 4: return k_enumerate<4>;
-        case 6: return k_enumerate<6>;
-        case 5: return k_enumerate<5>;
-        default: return k_enumerate<4>;
+        case 6: return last_loop ? k_enumerate<6, true> : k_enumerate<6, false>;
+        case 5: return last_loop ? k_enumerate<5, true> : k_enumerate<5, false>;
+        default: return last_loop ? k_enumerate<4, true> : k_enumerate<4, false>;
     }
 }
 }  // namespace
 
 int enum_blocks_per_sm(int warps_per_block, int occupancy) {
+    // The smaller residency of the two variants: a persistent grid must fit either.
     const size_t smem = enum_smem_bytes(warps_per_block);
-    EnumKernel k = enum_kernel(occupancy);
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, warps_per_block * 32, smem) != cudaSuccess) return 1;
-    return nb > 0 ? nb : 1;
+    int best = 1 << 30;
+    for (bool last_loop : {false, true}) {
+        EnumKernel k = enum_kernel(occupancy, last_loop);
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        int nb = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, warps_per_block * 32, smem) != cudaSuccess) return 1;
+        best = nb < best ? nb : best;
+    }
+    return best > 0 ? best : 1;
 }
 
 void launch_enumerate(const EnumParams &p, int blocks, int warps_per_block, int occupancy, cudaStream_t s) {
     const size_t smem = enum_smem_bytes(warps_per_block);
-    EnumKernel k = enum_kernel(occupancy);
+    EnumKernel k = enum_kernel(occupancy, p.last_loop != 0);
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k<<<blocks, warps_per_block * 32, smem, s>>>(p);
 }

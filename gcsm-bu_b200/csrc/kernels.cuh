@@ -109,6 +109,10 @@ struct EnumParams {
     unsigned long long time_limit_ns;  // >0: warps stop once the launch has run this long
     const unsigned int *abort_flag;  // nonzero: the batch update failed, skip enumeration
     const uint32_t *touched;         // bit per vertex: some batch key has it as list owner
+    // 1: some plan ends in a last level without a Cartesian tail, so the kernel variant with the
+    // register-resident last-level loop is launched (the other variant leaves that code out,
+    // which keeps the registers of the tail-counting paths).
+    uint32_t last_loop;
 };
 
 #define CSM_ROW_WORDS (1 + CSM_MAXQV)
