@@ -73,7 +73,7 @@ class CsmConfig(ctypes.Structure):
         ("replan_drift_pct", ctypes.c_int32),
         ("semi_bfs_items_per_warp", ctypes.c_int32),
         ("queue_slots", ctypes.c_int32),
-        ("reserved0", ctypes.c_int32),
+        ("inject_alloc_failure", ctypes.c_int32),
         ("time_limit_us", ctypes.c_uint64),
     ]
 

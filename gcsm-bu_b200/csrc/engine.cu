@@ -17,11 +17,6 @@ uint32_t bits_for(uint64_t v) {  // bits needed to represent 0..v
     return b;
 }
 
-template <typename T>
-cudaError_t dalloc(T **p, size_t count) {
-    return cudaMalloc((void **)p, sizeof(T) * (count ? count : 1));
-}
-
 }  // namespace
 
 // One-line description of a failed device consistency check (EnumControl.bad_*).
@@ -116,6 +111,7 @@ csm_status Engine::init() {
         qcap_ = 1u << 18;
     }
     time_limit_us_ = cfg_.time_limit_us;
+    inject_left_ = cfg_.inject_alloc_failure > 0 ? cfg_.inject_alloc_failure : 0;
     warps_per_block_ = cfg_.warps_per_block > 0 && cfg_.warps_per_block <= 8 ? cfg_.warps_per_block : 8;
     LaunchConfig lc;
     lc.strategy = opt_.search_strategy;
@@ -162,9 +158,9 @@ csm_status Engine::init() {
         tune_left_ = cfg_.autotune_batches;
         for (size_t i = 0; i < 2 * tune_cands_.size(); i++) CSM_CUDA(cudaEventCreate(&tune_ev_[i]));
     }
-    CSM_CUDA(dalloc(&d_ctrl_, 1));
+    CSM_CUDA(dev_alloc(&d_ctrl_, 1));
     CSM_CUDA(cudaMemset(d_ctrl_, 0, sizeof(EnumControl)));
-    CSM_CUDA(dalloc(&d_misc_, 8));
+    CSM_CUDA(dev_alloc(&d_misc_, 8));
     CSM_CUDA(cudaMallocHost(&h_counts_, sizeof(unsigned long long) * 64));
     CSM_CUDA(cudaMallocHost(&h_ctrl_, sizeof(EnumControl) * 2));
     return CSM_OK;
@@ -210,9 +206,11 @@ csm_status Engine::load_graph(uint32_t nv, const uint32_t *vlabel, uint64_t ne, 
     if (nv == 0 || !vlabel) return fail(CSM_ERR_INVALID_ARG, "empty vertex set");
     if (ne && (!src || !dst || !elabel)) return fail(CSM_ERR_INVALID_ARG, "null edge array");
     csm_status pst = prepare_tables(nv, vlabel, nullptr);
-    if (pst != CSM_OK) return pst;
     const uint32_t nvl = (uint32_t)vlab_raw_.size(), nel = (uint32_t)elab_raw_.size();
-    return build_lists(ne, src, dst, elabel, nvl, nel);
+    if (pst == CSM_OK) pst = build_lists(ne, src, dst, elabel, nvl, nel);
+    // A load that fails part way leaves device tables half built: later calls are refused.
+    if (pst != CSM_OK) poisoned_ = true;
+    return pst;
 }
 
 // Label spaces, relations, candidate-rule specs, key layout and the device tables of a graph
@@ -298,23 +296,23 @@ csm_status Engine::prepare_tables(uint32_t nv, const uint32_t *vlabel, const uin
         }
     }
     const size_t nmeta = (size_t)g_.R * nv;
-    CSM_CUDA(dalloc(&g_.vlab, nv));
+    CSM_CUDA(dev_alloc(&g_.vlab, nv));
     CSM_CUDA(cudaMemcpy(g_.vlab, vlab.data(), nv, cudaMemcpyHostToDevice));
-    CSM_CUDA(dalloc(&d_elab_raw_, nel));
+    CSM_CUDA(dev_alloc(&d_elab_raw_, nel));
     CSM_CUDA(cudaMemcpy(d_elab_raw_, elab_raw_.data(), sizeof(uint32_t) * nel, cudaMemcpyHostToDevice));
-    CSM_CUDA(dalloc(&d_rel_table_, rel_table_.size()));
+    CSM_CUDA(dev_alloc(&d_rel_table_, rel_table_.size()));
     CSM_CUDA(cudaMemcpy(d_rel_table_, rel_table_.data(), sizeof(uint16_t) * rel_table_.size(), cudaMemcpyHostToDevice));
-    CSM_CUDA(dalloc(&d_spec_begin_, nvl + 1));
+    CSM_CUDA(dev_alloc(&d_spec_begin_, nvl + 1));
     CSM_CUDA(cudaMemcpy(d_spec_begin_, spec_begin.data(), sizeof(uint32_t) * (nvl + 1), cudaMemcpyHostToDevice));
-    CSM_CUDA(dalloc(&d_specs_, specs.size()));
+    CSM_CUDA(dev_alloc(&d_specs_, specs.size()));
     if (!specs.empty())
         CSM_CUDA(cudaMemcpy(d_specs_, specs.data(), sizeof(NlfSpec) * specs.size(), cudaMemcpyHostToDevice));
-    CSM_CUDA(dalloc(&d_bits_, (size_t)nbitmaps_ * words_));
+    CSM_CUDA(dev_alloc(&d_bits_, (size_t)nbitmaps_ * words_));
     CSM_CUDA(cudaMemset(d_bits_, 0, sizeof(uint32_t) * (size_t)nbitmaps_ * words_));
-    CSM_CUDA(dalloc(&g_.meta, nmeta));
-    CSM_CUDA(dalloc(&g_.cap, nmeta));
-    CSM_CUDA(dalloc(&g_.pool_top, 1));
-    CSM_CUDA(dalloc(&d_touched_, words_));
+    CSM_CUDA(dev_alloc(&g_.meta, nmeta));
+    CSM_CUDA(dev_alloc(&g_.cap, nmeta));
+    CSM_CUDA(dev_alloc(&g_.pool_top, 1));
+    CSM_CUDA(dev_alloc(&d_touched_, words_));
     CSM_CUDA(cudaMemset(d_touched_, 0, sizeof(uint32_t) * words_));
     return CSM_OK;
 }
@@ -335,8 +333,8 @@ csm_status Engine::build_lists(uint64_t ne, const uint32_t *src, const uint32_t 
     std::string berr;
     do {
         cudaError_t e;
-        if ((e = dalloc(&d_src, ne)) || (e = dalloc(&d_dst, ne)) || (e = dalloc(&d_lab, ne)) ||
-            (e = dalloc(&k_raw, m)) || (e = dalloc(&k_sorted, m))) {
+        if ((e = dev_alloc(&d_src, ne)) || (e = dev_alloc(&d_dst, ne)) || (e = dev_alloc(&d_lab, ne)) ||
+            (e = dev_alloc(&k_raw, m)) || (e = dev_alloc(&k_sorted, m))) {
             st = cuda_fail(e, "initial edge buffers");
             break;
         }
@@ -347,7 +345,7 @@ csm_status Engine::build_lists(uint64_t ne, const uint32_t *src, const uint32_t 
             store_build_keys(ne, d_src, d_dst, d_lab, nullptr, lt, g_, kl_, k_raw, stream_);
         }
         store_sort_keys(nullptr, temp_bytes, k_raw, k_sorted, m, kl_, stream_);
-        if ((e = cudaMalloc(&temp, temp_bytes + 16))) {
+        if ((e = dev_alloc_bytes(&temp, temp_bytes + 16))) {
             st = cuda_fail(e, "sort scratch");
             break;
         }
@@ -364,7 +362,7 @@ csm_status Engine::build_lists(uint64_t ne, const uint32_t *src, const uint32_t 
                                                     : (unsigned long long)(10 * m64 + 64 * max_batch + (1u << 20));
         if (want > 0xFFFFFFF0ull) want = 0xFFFFFFF0ull;
         g_.pool_cap = want;
-        if ((e = dalloc(&g_.pool, g_.pool_cap))) {
+        if ((e = dev_alloc(&g_.pool, g_.pool_cap))) {
             st = cuda_fail(e, "adjacency pool");
             break;
         }
@@ -396,7 +394,7 @@ csm_status Engine::finish_load() {
     if (cfg_.replan_drift_pct > 0) {
         // Relation sizes at planning time, for the drift check after each batch.
         unsigned long long *d_sz = nullptr;
-        CSM_CUDA(dalloc(&d_sz, g_.R));
+        CSM_CUDA(dev_alloc(&d_sz, g_.R));
         CSM_CUDA(cudaMemsetAsync(d_sz, 0, sizeof(unsigned long long) * g_.R, stream_));
         store_rel_sizes(g_, d_sz, stream_);
         std::vector<unsigned long long> h(g_.R);
@@ -405,21 +403,21 @@ csm_status Engine::finish_load() {
         cudaFree(d_sz);
         rel_size_.assign(h.begin(), h.end());
         rel_size_planned_ = rel_size_;
-        CSM_CUDA(dalloc(&d_rel_delta_, g_.R));
+        CSM_CUDA(dev_alloc(&d_rel_delta_, g_.R));
         CSM_CUDA(cudaMallocHost(&h_rel_delta_, sizeof(long long) * g_.R));
     }
     const uint32_t np = (uint32_t)plans_.size();
-    CSM_CUDA(dalloc(&d_seed_lo_, 3 * (size_t)np));
-    CSM_CUDA(dalloc(&d_ticket_prefix_, np + 1));
-    CSM_CUDA(dalloc(&d_counts_, 2 * (size_t)np));
+    CSM_CUDA(dev_alloc(&d_seed_lo_, 3 * (size_t)np));
+    CSM_CUDA(dev_alloc(&d_ticket_prefix_, np + 1));
+    CSM_CUDA(dev_alloc(&d_counts_, 2 * (size_t)np));
     last_counts_.assign(2 * np, 0);
     cudaFreeHost(h_counts_);
     h_counts_ = nullptr;
     CSM_CUDA(cudaMallocHost(&h_counts_, sizeof(unsigned long long) * (2 * np + 32)));
     // Donation ring and the semi-BFS frontier.  The ring's slots are reused for the whole
     // launch, so it only needs room for the items in flight at once.
-    CSM_CUDA(dalloc(&d_queue_, qcap_));
-    CSM_CUDA(dalloc(&d_seq_, qcap_));
+    CSM_CUDA(dev_alloc(&d_queue_, qcap_));
+    CSM_CUDA(dev_alloc(&d_seq_, qcap_));
     CSM_CUDA(cudaMemset(d_seq_, 0, sizeof(unsigned long long) * qcap_));
     sc_.ctrl = d_ctrl_;
     sc_.queue = d_queue_;
@@ -430,12 +428,12 @@ csm_status Engine::finish_load() {
     const unsigned long long fbytes = cfg_.frontier_bytes ? cfg_.frontier_bytes : (1ull << 30);
     frontier_cap_ = std::max<unsigned long long>(1024, fbytes / 2 / sizeof(WorkItem));
     if (opt_.search_strategy >= 2 || cfg_.autotune_batches > 0) {
-        CSM_CUDA(dalloc(&d_frontier_[0], frontier_cap_));
-        CSM_CUDA(dalloc(&d_frontier_[1], frontier_cap_));
+        CSM_CUDA(dev_alloc(&d_frontier_[0], frontier_cap_));
+        CSM_CUDA(dev_alloc(&d_frontier_[1], frontier_cap_));
     }
     if (cfg_.materialize_rows) {
         row_cap_ = cfg_.materialize_rows;
-        CSM_CUDA(dalloc(&d_rows_, row_cap_ * CSM_ROW_WORDS));
+        CSM_CUDA(dev_alloc(&d_rows_, row_cap_ * CSM_ROW_WORDS));
     }
     csm_status bst = ensure_batch_capacity(cfg_.max_batch ? cfg_.max_batch : 65536);
     if (bst != CSM_OK) return bst;
@@ -460,7 +458,7 @@ csm_status Engine::compute_edge_stats(std::vector<EdgeStats> &stats) {
         return (uint32_t)(std::lower_bound(elab_raw_.begin(), elab_raw_.end(), raw) - elab_raw_.begin());
     };
     unsigned long long *d_stat = nullptr;
-    CSM_CUDA(dalloc(&d_stat, 2));
+    CSM_CUDA(dev_alloc(&d_stat, 2));
     stats.assign(queries_.size(), EdgeStats{});
     for (size_t qi = 0; qi < queries_.size(); qi++) {
         const Query &q = queries_[qi];
@@ -519,13 +517,13 @@ csm_status Engine::install_plans(const std::vector<EdgeStats> &stats) {
         terms.insert(terms.end(), hp.terms.begin(), hp.terms.end());
         dplans.push_back(hp.dev);
     }
-    if (!d_plans_) CSM_CUDA(dalloc(&d_plans_, dplans.size()));
+    if (!d_plans_) CSM_CUDA(dev_alloc(&d_plans_, dplans.size()));
     CSM_CUDA(cudaMemcpyAsync(d_plans_, dplans.data(), sizeof(DevPlan) * dplans.size(), cudaMemcpyHostToDevice, stream_));
     if (terms.size() > terms_cap_ || !d_terms_) {
         if (d_terms_) cudaFree(d_terms_);
         d_terms_ = nullptr;
         terms_cap_ = std::max<size_t>(terms.size(), 1);
-        CSM_CUDA(dalloc(&d_terms_, terms_cap_));
+        CSM_CUDA(dev_alloc(&d_terms_, terms_cap_));
     }
     if (!terms.empty())
         CSM_CUDA(cudaMemcpyAsync(d_terms_, terms.data(), sizeof(DevTailTerm) * terms.size(), cudaMemcpyHostToDevice,
@@ -616,7 +614,7 @@ uint64_t Engine::query_fingerprint() const {
 csm_status Engine::save_snapshot(const char *path) {
     if (!path) return fail(CSM_ERR_INVALID_ARG, "null path");
     if (!graph_loaded_) return fail(CSM_ERR_STATE, "load the data graph first");
-    if (poisoned_) return fail(CSM_ERR_STATE, "the engine failed an earlier batch; recreate it");
+    if (poisoned_) return fail(CSM_ERR_STATE, "the engine failed an earlier call (see its error); recreate it");
     CSM_CUDA(cudaSetDevice(device_));
     CSM_CUDA(cudaStreamSynchronize(stream_));
     unsigned long long used = 0;
@@ -662,12 +660,12 @@ csm_status Engine::load_snapshot(const char *path) {
         return fail(CSM_ERR_INVALID_ARG, "the snapshot was taken with other queries");
     if (h.V == 0 || h.used > h.capacity || h.capacity > 0xFFFFFFF0ull)
         return fail(CSM_ERR_INVALID_ARG, "corrupt snapshot header");
+    // Everything is read and validated before any device table is built, so a rejected file
+    // leaves the engine as it was (a good snapshot or load_graph may follow).
     std::vector<uint8_t> vlab(h.V);
     if (std::fread(vlab.data(), 1, h.V, fc.f) != h.V) return fail(CSM_ERR_INVALID_ARG, "truncated snapshot");
-    csm_status st = prepare_tables(h.V, nullptr, vlab.data());
-    if (st != CSM_OK) return st;
-    if (g_.R != h.R) return fail(CSM_ERR_INVALID_ARG, "the snapshot's relations differ from the queries'");
-    const size_t nmeta = (size_t)g_.R * g_.V;
+    if (h.R == 0 || (uint64_t)h.R * h.V > (1ull << 36)) return fail(CSM_ERR_INVALID_ARG, "corrupt snapshot header");
+    const size_t nmeta = (size_t)h.R * h.V;
     std::vector<uint2> meta(nmeta);
     std::vector<uint32_t> cap(nmeta), pool(h.used);
     if (std::fread(meta.data(), sizeof(uint2), nmeta, fc.f) != nmeta ||
@@ -685,54 +683,81 @@ csm_status Engine::load_snapshot(const char *path) {
             if ((l[j] >> 1) >= h.V || (l[j] & 1u) || (j && l[j] <= l[j - 1]))
                 return fail(CSM_ERR_INVALID_ARG, "corrupt snapshot adjacency list");
     }
+    csm_status st = prepare_tables(h.V, nullptr, vlab.data());
+    if (st == CSM_OK && g_.R != h.R)  // equal fingerprints give equal relations
+        st = fail(CSM_ERR_INVALID_ARG, "the snapshot's relations differ from the queries'");
+    if (st == CSM_OK) st = upload_snapshot(h.used, h.capacity, meta, cap, pool);
+    if (st != CSM_OK) poisoned_ = true;
+    return st;
+}
+
+// Device side of load_snapshot: the pool, the list table and the entries in use.
+csm_status Engine::upload_snapshot(uint64_t used, uint64_t capacity, const std::vector<uint2> &meta,
+                                   const std::vector<uint32_t> &cap, const std::vector<uint32_t> &pool) {
+    const size_t nmeta = meta.size();
     const uint64_t max_batch = cfg_.max_batch ? cfg_.max_batch : (1ull << 20);
-    unsigned long long want = cfg_.pool_entries ? cfg_.pool_entries : h.capacity;
-    want = std::max<unsigned long long>(want, h.used + 64 * max_batch + (1u << 20));
+    unsigned long long want = cfg_.pool_entries ? cfg_.pool_entries : capacity;
+    want = std::max<unsigned long long>(want, used + 64 * max_batch + (1u << 20));
     if (want > 0xFFFFFFF0ull) want = 0xFFFFFFF0ull;
     g_.pool_cap = want;
-    CSM_CUDA(dalloc(&g_.pool, g_.pool_cap));
+    CSM_CUDA(dev_alloc(&g_.pool, g_.pool_cap));
     CSM_CUDA(cudaMemcpy(g_.meta, meta.data(), sizeof(uint2) * nmeta, cudaMemcpyHostToDevice));
     CSM_CUDA(cudaMemcpy(g_.cap, cap.data(), sizeof(uint32_t) * nmeta, cudaMemcpyHostToDevice));
-    if (h.used) CSM_CUDA(cudaMemcpy(g_.pool, pool.data(), sizeof(uint32_t) * h.used, cudaMemcpyHostToDevice));
-    const unsigned long long top = h.used;
+    if (used) CSM_CUDA(cudaMemcpy(g_.pool, pool.data(), sizeof(uint32_t) * used, cudaMemcpyHostToDevice));
+    const unsigned long long top = used;
     CSM_CUDA(cudaMemcpy(g_.pool_top, &top, sizeof(top), cudaMemcpyHostToDevice));
     return finish_load();
 }
 
 csm_status Engine::ensure_batch_capacity(uint64_t n) {
     if (n <= batch_cap_) return CSM_OK;
-    clear_graphs();
-    graph_gen_++;
     uint64_t cap = std::max<uint64_t>(n, batch_cap_ * 2);
     if (2 * cap >= 0x7FFFFFFFull) return fail(CSM_ERR_LIMIT, "batch too large (limit 2^30 updates)");
+    const size_t m = 2 * cap;
+    // The new buffers are allocated first and replace the old ones only when all exist: a
+    // failed growth leaves the engine working at its previous capacity.
+    uint32_t *upd_src = nullptr, *upd_dst = nullptr, *upd_lab = nullptr, *pin = nullptr;
+    uint8_t *upd_del = nullptr;
+    unsigned long long *keys_raw = nullptr, *keys = nullptr;
+    void *sort_temp = nullptr;
+    BatchScratch b;
+    size_t tb = 0;
+    store_sort_keys(nullptr, tb, nullptr, nullptr, (uint32_t)m, kl_, stream_);
+    cudaError_t e;
+    if ((e = dev_alloc(&upd_src, cap)) || (e = dev_alloc(&upd_dst, cap)) || (e = dev_alloc(&upd_lab, cap)) ||
+        (e = dev_alloc(&upd_del, cap)) || (e = cudaMallocHost(&pin, sizeof(uint32_t) * 3 * cap + cap + 64)) ||
+        (e = dev_alloc(&keys_raw, m)) || (e = dev_alloc(&keys, m)) || (e = dev_alloc_bytes(&sort_temp, tb + 16)) ||
+        (e = dev_alloc(&b.eff, m)) || (e = dev_alloc(&b.heads, m)) || (e = dev_alloc(&b.nheads, 1)) ||
+        (e = dev_alloc(&b.seg_nins, m)) || (e = dev_alloc(&b.seg_ndel, m)) || (e = dev_alloc(&b.seg_end, m)) ||
+        (e = dev_alloc(&b.scr_y, m)) || (e = dev_alloc(&b.scr_lb, m)) || (e = dev_alloc(&b.counters, 2)) ||
+        (e = dev_alloc(&b.error, 1))) {
+        void *got[] = {upd_src, upd_dst, upd_lab, upd_del, keys_raw, keys, sort_temp, b.eff, b.heads, b.nheads,
+                       b.seg_nins, b.seg_ndel, b.seg_end, b.scr_y, b.scr_lb, b.counters, b.error};
+        for (void *p : got)
+            if (p) cudaFree(p);
+        if (pin) cudaFreeHost(pin);
+        cudaGetLastError();
+        return cuda_fail(e, "batch buffers");
+    }
     CSM_CUDA(cudaStreamSynchronize(stream_));
+    clear_graphs();
+    graph_gen_++;
     void *old[] = {d_upd_src_, d_upd_dst_, d_upd_lab_, d_upd_del_, d_keys_raw_, d_keys_, d_sort_temp_, bs_.eff,
                    bs_.heads, bs_.nheads, bs_.seg_nins, bs_.seg_ndel, bs_.seg_end, bs_.scr_y, bs_.scr_lb, bs_.counters,
                    bs_.error};
     for (void *p : old)
         if (p) cudaFree(p);
     if (h_pin_) cudaFreeHost(h_pin_);
-    const size_t m = 2 * cap;
-    CSM_CUDA(dalloc(&d_upd_src_, cap));
-    CSM_CUDA(dalloc(&d_upd_dst_, cap));
-    CSM_CUDA(dalloc(&d_upd_lab_, cap));
-    CSM_CUDA(dalloc(&d_upd_del_, cap));
-    CSM_CUDA(cudaMallocHost(&h_pin_, sizeof(uint32_t) * 3 * cap + cap + 64));
-    CSM_CUDA(dalloc(&d_keys_raw_, m));
-    CSM_CUDA(dalloc(&d_keys_, m));
-    sort_temp_bytes_ = 0;
-    store_sort_keys(nullptr, sort_temp_bytes_, d_keys_raw_, d_keys_, (uint32_t)m, kl_, stream_);
-    CSM_CUDA(cudaMalloc(&d_sort_temp_, sort_temp_bytes_ + 16));
-    CSM_CUDA(dalloc(&bs_.eff, m));
-    CSM_CUDA(dalloc(&bs_.heads, m));
-    CSM_CUDA(dalloc(&bs_.nheads, 1));
-    CSM_CUDA(dalloc(&bs_.seg_nins, m));
-    CSM_CUDA(dalloc(&bs_.seg_ndel, m));
-    CSM_CUDA(dalloc(&bs_.seg_end, m));
-    CSM_CUDA(dalloc(&bs_.scr_y, m));
-    CSM_CUDA(dalloc(&bs_.scr_lb, m));
-    CSM_CUDA(dalloc(&bs_.counters, 2));
-    CSM_CUDA(dalloc(&bs_.error, 1));
+    d_upd_src_ = upd_src;
+    d_upd_dst_ = upd_dst;
+    d_upd_lab_ = upd_lab;
+    d_upd_del_ = upd_del;
+    h_pin_ = pin;
+    d_keys_raw_ = keys_raw;
+    d_keys_ = keys;
+    d_sort_temp_ = sort_temp;
+    sort_temp_bytes_ = tb;
+    bs_ = b;
     batch_cap_ = cap;
     return CSM_OK;
 }
@@ -764,7 +789,7 @@ csm_status Engine::apply_host_ctx(const ExecContext &ctx, uint64_t n, const uint
 csm_status Engine::apply_host_on(cudaStream_t s, uint64_t n, const uint32_t *src, const uint32_t *dst,
                                  const uint32_t *elabel, const uint8_t *is_delete, csm_batch_result *out) {
     if (!graph_loaded_) return fail(CSM_ERR_STATE, "load the data graph first");
-    if (poisoned_) return fail(CSM_ERR_STATE, "the engine failed an earlier batch; recreate it");
+    if (poisoned_) return fail(CSM_ERR_STATE, "the engine failed an earlier call (see its error); recreate it");
     if (n && (!src || !dst || !elabel)) return fail(CSM_ERR_INVALID_ARG, "null update array");
     csm_status st = ensure_batch_capacity(n);
     if (st != CSM_OK) return st;
@@ -786,7 +811,7 @@ csm_status Engine::apply_host_on(cudaStream_t s, uint64_t n, const uint32_t *src
 csm_status Engine::apply_device(uint64_t n, const uint32_t *src, const uint32_t *dst, const uint32_t *elabel,
                                 const uint8_t *is_delete, cudaStream_t stream, csm_batch_result *out) {
     if (!graph_loaded_) return fail(CSM_ERR_STATE, "load the data graph first");
-    if (poisoned_) return fail(CSM_ERR_STATE, "the engine failed an earlier batch; recreate it");
+    if (poisoned_) return fail(CSM_ERR_STATE, "the engine failed an earlier call (see its error); recreate it");
     if (n && (!src || !dst || !elabel)) return fail(CSM_ERR_INVALID_ARG, "null update array");
     csm_status st = ensure_batch_capacity(n);
     if (st != CSM_OK) return st;
@@ -808,7 +833,7 @@ csm_status Engine::apply_device_noalloc(uint64_t n, const uint32_t *src, const u
                                         const uint8_t *is_delete, cudaStream_t stream, const EnumScratch &scratch,
                                         csm_batch_result *out) {
     if (!graph_loaded_) return fail(CSM_ERR_STATE, "load the data graph first");
-    if (poisoned_) return fail(CSM_ERR_STATE, "the engine failed an earlier batch; recreate it");
+    if (poisoned_) return fail(CSM_ERR_STATE, "the engine failed an earlier call (see its error); recreate it");
     if (n && (!src || !dst || !elabel)) return fail(CSM_ERR_INVALID_ARG, "null update array");
     if (n > batch_cap_)
         return fail(CSM_ERR_LIMIT, "batch of " + std::to_string(n) + " updates exceeds the " +
@@ -1003,7 +1028,10 @@ csm_status Engine::run_batch(uint64_t n, const uint32_t *src, const uint32_t *ds
         }
         stats_.pool_used = g_.pool_cap;
         csm_status cst = maybe_compact(s);
-        if (cst != CSM_OK) return cst;
+        if (cst != CSM_OK) {
+            poisoned_ = true;  // this batch's lists are only partly merged
+            return cst;
+        }
         CSM_CUDA(cudaMemsetAsync(bs_.error, 0, sizeof(unsigned int), s));
         CSM_CUDA(cudaMemsetAsync(d_counts_ + np, 0, sizeof(unsigned long long) * np, s));
         store_insert(m, d_keys_, kl_, g_, bs_, s);
@@ -1077,8 +1105,10 @@ csm_status Engine::run_batch(uint64_t n, const uint32_t *src, const uint32_t *ds
         const csm_status rst = maybe_replan();
         if (rst != CSM_OK) return rst;
     }
-    const csm_status cst = maybe_compact(s);
-    return cst != CSM_OK ? cst : deferred_;
+    // The batch is applied: a compaction that cannot run now (no memory for the new layout) is
+    // retried after the next batch, and a pool that then overflows takes the rerun path.
+    if (maybe_compact(s) != CSM_OK && poisoned_) return CSM_ERR_CUDA;
+    return deferred_;
 }
 
 csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
@@ -1172,6 +1202,13 @@ csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
                 CSM_CUDA(record_event(ev_[3 + 2 * ph], s));
                 return CSM_OK;
             }
+            // This expansion launch's work counters, before the next launch's control block
+            // replaces them (the batch's final launch is added when the batch completes).
+            stats_.enum_scan_entries += h_ctrl_[ph].scan_entries;
+            stats_.enum_probes += h_ctrl_[ph].probes;
+            stats_.enum_tail_lists += h_ctrl_[ph].tail_lists;
+            stats_.donations += h_ctrl_[ph].donations;
+            stats_.donations_refused += h_ctrl_[ph].queue_full;
             const bool grew = rows_out != nfront || frontier == nullptr;
             frontier = d_frontier_[buf];
             nfront = rows_out;
@@ -1232,12 +1269,12 @@ csm_status Engine::maybe_compact(cudaStream_t s) {
     unsigned long long want = g_.pool_cap;
     if (!roomy(want)) want = std::min(limit, std::max(want * 2, 2 * (total + headroom)));
     uint32_t *np = nullptr;
-    e = total <= want ? cudaMalloc(&np, sizeof(uint32_t) * want) : cudaErrorMemoryAllocation;
+    e = total <= want ? dev_alloc(&np, want) : cudaErrorMemoryAllocation;
     if (e == cudaErrorMemoryAllocation && want > g_.pool_cap && total <= g_.pool_cap) {
         // No memory to grow: a same-size pool still recovers the slack of relocated lists.
         cudaGetLastError();
         want = g_.pool_cap;
-        e = cudaMalloc(&np, sizeof(uint32_t) * want);
+        e = dev_alloc(&np, want);
     }
     if (e != cudaSuccess) {
         cudaGetLastError();

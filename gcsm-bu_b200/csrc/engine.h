@@ -130,6 +130,22 @@ class Engine {
 
   private:
     csm_status ensure_batch_capacity(uint64_t n);
+    csm_status upload_snapshot(uint64_t used, uint64_t capacity, const std::vector<uint2> &meta,
+                               const std::vector<uint32_t> &cap, const std::vector<uint32_t> &pool);
+    // Every device allocation of the engine.  With csm_config.inject_alloc_failure = N > 0 the
+    // N-th one fails as out of memory (once): fault injection for the error paths.
+    cudaError_t dev_alloc_bytes(void **p, size_t bytes) {
+        if (inject_left_ > 0 && --inject_left_ == 0) {
+            *p = nullptr;
+            return cudaErrorMemoryAllocation;
+        }
+        return cudaMalloc(p, bytes ? bytes : 1);
+    }
+    template <typename T>
+    cudaError_t dev_alloc(T **p, size_t count) {
+        return dev_alloc_bytes(reinterpret_cast<void **>(p), sizeof(T) * (count ? count : 1));
+    }
+    int64_t inject_left_ = 0;
     csm_status run_batch(uint64_t n, const uint32_t *src, const uint32_t *dst, const uint32_t *elabel,
                          const uint8_t *is_delete, bool has_delete, cudaStream_t s, csm_batch_result *out);
     csm_status enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s);

@@ -640,7 +640,9 @@ __device__ bool count_last_packed(WarpState &S, const EnumParams &P, const DevPl
             s_off = ms.x;
             s_sz = ms.y;
         }
-        if (sib_b != 0xFFu && s_sz <= sh_min) {
+        // The smallest list is the pivot, the lowest backward-neighbour index on ties (the
+        // choice enter_level makes), so the work counters do not depend on packing.
+        if (sib_b != 0xFFu && (s_sz < sh_min || (s_sz == sh_min && sib_b < sh_piv))) {
             pv = sib_b;
             p_off = s_off;
             p_len = s_sz;

@@ -84,7 +84,8 @@ typedef struct csm_config {
                                        frontier holds this many items per warp; 0 = 512 */
     int32_t queue_slots;            /* work-donation ring of the enumeration: slots, a power of two
                                        in [32, 2^24]; 0 = 2^18 (a full ring only costs balance) */
-    int32_t reserved0;
+    int32_t inject_alloc_failure;   /* >0: the engine's N-th device allocation fails as out of memory
+                                       (once); fault injection for testing callers' error paths */
     uint64_t time_limit_us;         /* >0: every enumeration launch stops after this many
                                        microseconds; see csm_set_time_limit */
 } csm_config;

@@ -15,7 +15,7 @@ int main(void) {
     F(csm_config, blocks_per_sm); F(csm_config, warps_per_block); F(csm_config, steal_chunk);
     F(csm_config, occupancy); F(csm_config, autotune_batches); F(csm_config, cuda_graphs);
     F(csm_config, replan_drift_pct); F(csm_config, semi_bfs_items_per_warp);
-    F(csm_config, queue_slots); F(csm_config, reserved0); F(csm_config, time_limit_us);
+    F(csm_config, queue_slots); F(csm_config, inject_alloc_failure); F(csm_config, time_limit_us);
     F(csm_batch_result, positive); F(csm_batch_result, negative); F(csm_batch_result, inserted);
     F(csm_batch_result, deleted); F(csm_batch_result, latency_ns); F(csm_batch_result, apply_ns);
     F(csm_batch_result, enum_ns);

@@ -245,3 +245,26 @@ def test_snapshot_restore_continues_stream(tmp_path):
         c.load_snapshot(snap)
     for e in (a, b_eng, c):
         e.close()
+
+
+def test_work_counters_do_not_depend_on_the_schedule():
+    """The roofline's algorithmic bytes come from the kernel's work counters (pivot entries
+    scanned, membership probes, tail lists): per expanded partial embedding, never per launch or
+    per warp, so they are the same under every search strategy, launch shape and donation
+    granularity for the same batches."""
+    w = small_workload("c2", scale=0.01, batch=1500, nqueries=6)
+    seen = {}
+    for cfg in (dict(search_strategy=0), dict(search_strategy=1), dict(search_strategy=2),
+                dict(search_strategy=3), dict(search_strategy=0, warps_per_block=4, steal_chunk=8),
+                dict(search_strategy=2, semi_bfs_items_per_warp=8)):
+        with csm.Engine(**cfg) as eng:
+            for q in w.queries:
+                eng.load_query(q)
+            eng.load_graph(w.data)
+            counts = [[(r.positive, r.negative) for r in eng.apply(b)] for b in w.batches[:3]]
+            st = eng.stats()
+            seen[str(cfg)] = (counts, st.enum_scan_entries, st.enum_probes, st.enum_tail_lists)
+    first = next(iter(seen.values()))
+    assert first[1] > 0 and first[2] > 0
+    for k, v in seen.items():
+        assert v == first, k
