@@ -829,7 +829,7 @@ __device__ unsigned long long count_last_level(WarpState &S, const EnumParams &P
 // Runs one work item to completion (or until the device clock passes `deadline`, when that is
 // nonzero: the rest of the item is then dropped and CSM_ERRBIT_TIMEOUT set).  Returns the number
 // of matches counted.
-template <bool LASTLOOP>
+template <bool LASTLOOP, int MODE>
 __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, uint32_t &scans,
                                        uint32_t &probes, uint32_t &tails, unsigned int &err,
                                        unsigned long long deadline) {
@@ -840,7 +840,7 @@ __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, uint32
     const uint32_t L0 = S.item_depth == 0 ? 1u : S.item_depth;
     unsigned long long cnt = 0;
 
-    if (P.mode == CSM_ENUM_MODE_EXPAND && L0 + 1 >= E) {
+    if (MODE == CSM_ENUM_MODE_EXPAND && L0 + 1 >= E) {
         // Nothing left to expand before the counting level: pass the item through.
         unsigned long long r = 0;
         if (lane == 0) r = atomicAdd(&P.ctrl->out_rows, 1ull);
@@ -900,7 +900,7 @@ __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, uint32
         }
         if (S.pos[d] < S.nbuf[d]) {
             // Siblings whose subtree is only the last level: count them together.
-            if (d + 2 == n && E == n && d >= 2 && P.mode == CSM_ENUM_MODE_COUNT &&
+            if (d + 2 == n && E == n && d >= 2 && MODE == CSM_ENUM_MODE_COUNT &&
                 count_last_packed(S, P, pl, d, cnt, scans, probes))
                 continue;
             // Descend into the next buffered candidate.
@@ -931,7 +931,7 @@ __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, uint32
             d--;
             continue;
         }
-        if (LASTLOOP && d + 1 == n && E == n && d >= 2 && P.mode == CSM_ENUM_MODE_COUNT && S.nbn[d] <= kLastLists + 1) {
+        if (LASTLOOP && d + 1 == n && E == n && d >= 2 && MODE == CSM_ENUM_MODE_COUNT && S.nbn[d] <= kLastLists + 1) {
             cnt += count_last_level(S, P, pl, L0, d, scans, probes, err, deadline);
             if (err & CSM_ERRBIT_TIMEOUT) break;
             continue;
@@ -1024,7 +1024,7 @@ __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, uint32
         if (lane == 0) S.lo[d] += 32u;
         const uint32_t mask = __ballot_sync(0xffffffffu, ok);
         const uint32_t rank = __popc(mask & ((1u << lane) - 1u));
-        if (P.mode == CSM_ENUM_MODE_EXPAND && d == L0) {
+        if (MODE == CSM_ENUM_MODE_EXPAND && d == L0) {
             // One BFS level: survivors become items of depth d + 1.
             const uint32_t c = __popc(mask);
             unsigned long long r = 0;
@@ -1101,7 +1101,7 @@ __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, uint32
             cnt += t;
             tails += __popc(mask);
         } else if (d + 1 == n) {
-            if (P.mode == CSM_ENUM_MODE_ROWS) {
+            if (MODE == CSM_ENUM_MODE_ROWS) {
                 const uint32_t c = __popc(mask);
                 unsigned long long r = 0;
                 if (lane == 0 && c) r = atomicAdd(&P.ctrl->out_rows, (unsigned long long)c);
@@ -1136,7 +1136,9 @@ __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, uint32
 }
 
 // MINB resident blocks of 256 threads per SM: the register budget per thread follows from it.
-template <int MINB, bool LASTLOOP>
+// MODE: CSM_ENUM_MODE_* of the launch (each variant holds only its mode's code, which keeps the
+// hot loop's instruction footprint small).
+template <int MINB, bool LASTLOOP, int MODE>
 __global__ void __launch_bounds__(256, MINB) k_enumerate(EnumParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
     WarpState &S = reinterpret_cast<WarpState *>(smem)[threadIdx.x >> 5];
@@ -1205,7 +1207,7 @@ __global__ void __launch_bounds__(256, MINB) k_enumerate(EnumParams P) {
                 break;
             }
         }
-        const unsigned long long c = run_item<LASTLOOP>(S, P, scans, probes, tails, err, deadline);
+        const unsigned long long c = run_item<LASTLOOP, MODE>(S, P, scans, probes, tails, err, deadline);
         if (lane == 0 && c) atomicAdd(P.counts + S.item_plan, c);
         if ((scans | probes | tails) >= (1u << 30)) {
             atomicAdd(&P.ctrl->scan_entries, (unsigned long long)scans);
@@ -1327,21 +1329,28 @@ size_t enum_smem_bytes(int warps_per_block) { return sizeof(WarpState) * (size_t
 
 namespace {
 using EnumKernel = void (*)(EnumParams);
-EnumKernel enum_kernel(int occupancy, bool last_loop) {
+template <int MINB>
+EnumKernel enum_kernel_mode(bool last_loop, uint32_t mode) {
+    if (mode == CSM_ENUM_MODE_EXPAND) return k_enumerate<MINB, false, CSM_ENUM_MODE_EXPAND>;
+    if (mode == CSM_ENUM_MODE_ROWS) return k_enumerate<MINB, false, CSM_ENUM_MODE_ROWS>;
+    return last_loop ? k_enumerate<MINB, true, CSM_ENUM_MODE_COUNT> : k_enumerate<MINB, false, CSM_ENUM_MODE_COUNT>;
+}
+
+EnumKernel enum_kernel(int occupancy, bool last_loop, uint32_t mode) {
     switch (occupancy) {
-        case 6: return last_loop ? k_enumerate<6, true> : k_enumerate<6, false>;
-        case 5: return last_loop ? k_enumerate<5, true> : k_enumerate<5, false>;
-        default: return last_loop ? k_enumerate<4, true> : k_enumerate<4, false>;
+        case 6: return enum_kernel_mode<6>(last_loop, mode);
+        case 5: return enum_kernel_mode<5>(last_loop, mode);
+        default: return enum_kernel_mode<4>(last_loop, mode);
     }
 }
 }  // namespace
 
 int enum_blocks_per_sm(int warps_per_block, int occupancy) {
-    // The smaller residency of the two variants: a persistent grid must fit either.
+    // The smallest residency of the variants: a persistent grid must fit each of them.
     const size_t smem = enum_smem_bytes(warps_per_block);
     int best = 1 << 30;
-    for (bool last_loop : {false, true}) {
-        EnumKernel k = enum_kernel(occupancy, last_loop);
+    for (int v = 0; v < 4; v++) {
+        EnumKernel k = enum_kernel(occupancy, v == 1, v < 2 ? CSM_ENUM_MODE_COUNT : (uint32_t)(v - 1));
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         int nb = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, warps_per_block * 32, smem) != cudaSuccess) return 1;
@@ -1352,7 +1361,7 @@ int enum_blocks_per_sm(int warps_per_block, int occupancy) {
 
 void launch_enumerate(const EnumParams &p, int blocks, int warps_per_block, int occupancy, cudaStream_t s) {
     const size_t smem = enum_smem_bytes(warps_per_block);
-    EnumKernel k = enum_kernel(occupancy, p.last_loop != 0);
+    EnumKernel k = enum_kernel(occupancy, p.last_loop != 0, p.mode);
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k<<<blocks, warps_per_block * 32, smem, s>>>(p);
 }
