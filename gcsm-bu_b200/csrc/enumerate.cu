@@ -713,6 +713,7 @@ __device__ bool count_last_packed(WarpState &S, const EnumParams &P, const DevPl
 // of the remaining range) and checks the time limit.  Returns the count; the level is left
 // exhausted (S.lo[d] >= S.hi[d]).
 constexpr uint32_t kLastLists = 1;
+constexpr uint32_t kWindows = 3;
 
 __device__ unsigned long long count_last_level(WarpState &S, const EnumParams &P, const DevPlan *pl, uint32_t L0,
                                                uint32_t d, uint32_t &scans, uint32_t &probes, unsigned int &err,
@@ -768,17 +769,30 @@ __device__ unsigned long long count_last_level(WarpState &S, const EnumParams &P
 #pragma unroll
         for (uint32_t j = 0; j < kLastLists; j++) {
             if (j >= nl) break;
-            const uint32_t below = __ballot_sync(0xffffffffu, win[j] < key_hi);
-            uint32_t e = 0xFFFFFFFFu, nhi;
-            if (below != 0xffffffffu) {
-                nhi = l_cur[j] + __popc(below);
-                const uint32_t pos = shfl_lower_bound(win[j], cand << 1);
-                const uint32_t got = __shfl_sync(0xffffffffu, win[j], pos);
+            uint32_t e = 0xFFFFFFFFu, nhi = 0;
+            // The chunk's candidates span ~40-55 entries of the other list on the measured
+            // queries: walk up to kWindows consecutive 32-entry windows (one coalesced load each)
+            // before bracketing the rest of the list with the warp search.
+            const uint32_t *L = P.g.pool + l_off[j];
+            uint32_t c0 = l_cur[j], w = win[j];
+            bool done = false;
+#pragma unroll 1
+            for (uint32_t k = 0; k < kWindows; k++) {
+                const uint32_t below = __ballot_sync(0xffffffffu, w < key_hi);
+                const uint32_t pos = shfl_lower_bound(w, cand << 1);
+                const uint32_t got = __shfl_sync(0xffffffffu, w, pos);
                 if ((got >> 1) == cand && got != 0xFFFFFFFFu) e = got;
-            } else {
-                const uint32_t *L = P.g.pool + l_off[j];
-                nhi = warp_lower_bound(L, l_cur[j] + 32, l_size[j], key_hi, lane);
-                if (ok) e = find_entry(L + l_cur[j], nhi - l_cur[j], cand);
+                if (below != 0xffffffffu) {
+                    nhi = c0 + __popc(below);
+                    done = true;
+                    break;
+                }
+                c0 += 32;
+                w = c0 + lane < l_size[j] ? __ldg(L + c0 + lane) : 0xFFFFFFFFu;
+            }
+            if (!done) {
+                nhi = warp_lower_bound(L, c0, l_size[j], key_hi, lane);
+                if (ok && e == 0xFFFFFFFFu) e = find_entry(L + c0, nhi - c0, cand);
             }
             if (ok) {
                 probes++;
