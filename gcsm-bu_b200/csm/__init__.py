@@ -96,7 +96,7 @@ class CsmStats(ctypes.Structure):
         "batches", "enum_launches", "kernel_launches", "enum_scan_entries", "enum_probes",
         "enum_tail_lists", "donations", "enum_ns", "apply_ns", "pool_used", "pool_capacity",
         "compactions", "tuned_strategy", "tuned_steal_chunk", "tuned_warps_per_block", "tuned_occupancy",
-        "graph_launches", "replans", "donations_refused")] + [("reserved", ctypes.c_uint64 * 1)]
+        "graph_launches", "replans", "donations_refused", "enum_shared_last")]
 
 
 class CsmError(RuntimeError):

@@ -98,6 +98,15 @@ struct DevPlan {
     uint32_t nterms;
     DevLevel lv[CSM_MAXQV];
     DevTail tail;
+    // 1 when there is no tail and the last query vertex has no backward neighbour at depth
+    // n - 2: its candidates then depend only on the prefix f[0..n-3], so they are counted once
+    // per such prefix, and each vertex at depth n - 2 subtracts one when it is itself one of
+    // them (injectivity; possible only when the two query vertices share a label).
+    uint8_t shared_last;
+    // Items of this depth or deeper pass a breadth-first expansion unexpanded: tail_start - 1,
+    // or n - 2 for shared_last plans (whose level n - 2 stays whole inside one item).
+    uint8_t expand_stop;
+    uint8_t pad2[2];
 };
 
 // Work item of the persistent enumeration: a partial embedding with `depth` fixed vertices
@@ -136,6 +145,7 @@ struct EnumControl {
     unsigned long long expand_bound;  // upper bound of the next BFS level
     unsigned long long t_start;       // device clock (ns) when the launch's control block was reset
     unsigned long long queue_full;    // donations refused because the ring was full
+    unsigned long long shared_last;   // last levels counted once for a prefix (DevPlan.shared_last)
     // First failed consistency check of the launch (CSM_ERRBIT_CORRUPT): where (CSM_BAD_*) and
     // three values describing it.  The offending item, list or entry is skipped, not used.
     unsigned int bad_where;

@@ -1067,6 +1067,7 @@ csm_status Engine::run_batch(uint64_t n, const uint32_t *src, const uint32_t *ds
         stats_.enum_tail_lists += c.tail_lists;
         stats_.donations += c.donations;
         stats_.donations_refused += c.queue_full;
+        stats_.enum_shared_last += c.shared_last;
         if (c.error & CSM_ERRBIT_CORRUPT) {
             poisoned_ = true;
             return fail(CSM_ERR_STATE, describe_bad(c));
@@ -1209,6 +1210,7 @@ csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
             stats_.enum_tail_lists += h_ctrl_[ph].tail_lists;
             stats_.donations += h_ctrl_[ph].donations;
             stats_.donations_refused += h_ctrl_[ph].queue_full;
+            stats_.enum_shared_last += h_ctrl_[ph].shared_last;
             const bool grew = rows_out != nfront || frontier == nullptr;
             frontier = d_frontier_[buf];
             nfront = rows_out;

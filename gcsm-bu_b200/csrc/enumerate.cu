@@ -67,6 +67,10 @@ struct __align__(16) WarpState {
     uint32_t item_depth;
     uint32_t item_lo;
     uint32_t item_hi;
+    // Shared last level (DevPlan.shared_last): its candidate count for the current prefix
+    // f[0..n-3], and whether it is being counted (1) or known (2).
+    unsigned long long sl_count;
+    uint32_t sl_state;
 };
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
@@ -446,7 +450,10 @@ __device__ void publish_item(const EnumParams &P, uint32_t pos, uint32_t plan, u
 __device__ bool try_donate(WarpState &S, const EnumParams &P, const DevPlan *pl, uint32_t L0, uint32_t d) {
     const uint32_t lane = lane_id();
     const uint32_t E = pl->tail_start;
-    for (uint32_t l = L0; l <= d; l++) {
+    // A shared last level is counted once per prefix at depth n - 3: the two deepest levels of
+    // a prefix stay with the warp that holds it (so neither is counted twice).
+    const uint32_t top = pl->shared_last ? pl->n - 3u : d;
+    for (uint32_t l = L0; l <= d && l <= top; l++) {
         const uint32_t lo = S.lo[l], hi = S.hi[l];
         const uint32_t minr = (l == 1) ? 64u : P.steal_min;
         if (hi > lo && hi - lo >= minr) {
@@ -840,12 +847,44 @@ __device__ unsigned long long count_last_level(WarpState &S, const EnumParams &P
     return cnt;
 }
 
+// Shared last level (DevPlan.shared_last), level d = n - 2 with candidates buffered: the count
+// of the last level for the prefix f[0..n-3] was taken once (S.sl_count, with f[n-2] left out of
+// its exclusions), so each buffered candidate v contributes that count, minus one when v is
+// itself a candidate of the last level — in every backward list of level n - 1 under the flag
+// rule and in its NLF bitmap.  v differs from every prefix vertex of its own label already, so
+// nothing else changes.  Consumes the buffer.
+__device__ unsigned long long count_shared_last(WarpState &S, const EnumParams &P, const DevPlan *pl, uint32_t d,
+                                                uint32_t &probes) {
+    const uint32_t lane = lane_id();
+    const uint32_t L = d + 1;
+    const uint32_t ps = S.pos[d], k = S.nbuf[d] - ps;
+    unsigned long long total = (unsigned long long)k * S.sl_count;
+    if ((__ldg(&pl->lv[L].excl_mask) >> d) & 1u) {
+        bool in = lane < k;
+        if (in) {
+            const uint32_t v = S.buf[d][ps + lane];
+            const uint32_t nbn = S.nbn[L], bb = S.bnb[L], oldm = S.oldm[L], nlf_id = S.nlf[L];
+            for (uint32_t b = 0; in && b < nbn; b++) {
+                const uint32_t e = find_entry(P.g.pool + S.poff[bb + b], S.psz[bb + b], v);
+                probes++;
+                in = e != 0xFFFFFFFFu && !(((oldm >> b) & 1u) && (e & 1u));
+            }
+            if (in && nlf_id != CSM_NO_BITMAP) in = test_bit(bitmap(P, nlf_id), v);
+        }
+        total -= __popc(__ballot_sync(0xffffffffu, in));
+    }
+    __syncwarp();
+    if (lane == 0) S.pos[d] = S.nbuf[d];
+    __syncwarp();
+    return total;
+}
+
 // Runs one work item to completion (or until the device clock passes `deadline`, when that is
 // nonzero: the rest of the item is then dropped and CSM_ERRBIT_TIMEOUT set).  Returns the number
 // of matches counted.
 template <bool LASTLOOP, int MODE>
 __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, uint32_t &scans,
-                                       uint32_t &probes, uint32_t &tails, unsigned int &err,
+                                       uint32_t &probes, uint32_t &tails, uint32_t &shared, unsigned int &err,
                                        unsigned long long deadline) {
     const uint32_t lane = lane_id();
     const DevPlan *pl = P.plans + S.item_plan;
@@ -854,7 +893,7 @@ __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, uint32
     const uint32_t L0 = S.item_depth == 0 ? 1u : S.item_depth;
     unsigned long long cnt = 0;
 
-    if (MODE == CSM_ENUM_MODE_EXPAND && L0 + 1 >= E) {
+    if (MODE == CSM_ENUM_MODE_EXPAND && L0 >= pl->expand_stop) {
         // Nothing left to expand before the counting level: pass the item through.
         unsigned long long r = 0;
         if (lane == 0) r = atomicAdd(&P.ctrl->out_rows, 1ull);
@@ -888,6 +927,8 @@ __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, uint32
     }
     uint32_t d = L0;
     uint32_t iter = 0;
+    unsigned long long sl_before = 0;
+    if (lane == 0) S.sl_state = 0;
     const uint32_t *nlf0 = bitmap(P, pl->nlf0);
     const uint32_t *nlf1 = bitmap(P, pl->nlf1);
 
@@ -913,6 +954,24 @@ __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, uint32
             if (granted && !try_donate(S, P, pl, L0, d) && lane == 0) atomicAdd(&P.ctrl->hungry, 1u);
         }
         if (S.pos[d] < S.nbuf[d]) {
+            if (MODE == CSM_ENUM_MODE_COUNT && d + 2 == n && pl->shared_last) {
+                // The last level does not depend on these candidates: count it once for the
+                // prefix (first time here), then settle every buffered candidate at once.
+                if (S.sl_state == 2) {
+                    cnt += count_shared_last(S, P, pl, d, probes);
+                    continue;
+                }
+                sl_before = cnt;
+                shared++;
+                d++;
+                enter_level(S, P, pl, d, 0, 0xFFFFFFFFu);
+                if (lane == 0) {
+                    S.sl_state = 1;
+                    S.exm[d] &= (uint16_t)~(1u << (d - 1));  // f[n-2] is settled per candidate
+                }
+                __syncwarp();
+                continue;
+            }
             // Siblings whose subtree is only the last level: count them together.
             if (d + 2 == n && E == n && d >= 2 && MODE == CSM_ENUM_MODE_COUNT &&
                 count_last_packed(S, P, pl, d, cnt, scans, probes))
@@ -936,11 +995,21 @@ __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, uint32
                 tails++;
             } else {
                 d++;
+                if (lane == 0 && d + 2 == n) S.sl_state = 0;  // a new prefix f[0..n-3]
                 enter_level(S, P, pl, d, 0, 0xFFFFFFFFu);
             }
             continue;
         }
         if (S.lo[d] >= S.hi[d]) {
+            if (MODE == CSM_ENUM_MODE_COUNT && d + 1 == n && S.sl_state == 1) {
+                // The shared last level is counted: keep its count for the candidates above.
+                if (lane == 0) {
+                    S.sl_count = cnt - sl_before;
+                    S.sl_state = 2;
+                }
+                cnt = sl_before;
+                __syncwarp();
+            }
             if (d == L0) break;
             d--;
             continue;
@@ -1160,7 +1229,7 @@ __global__ void __launch_bounds__(256, MINB) k_enumerate(EnumParams P) {
     if (P.abort_flag != nullptr && *(volatile const unsigned int *)P.abort_flag) return;
     // Per-lane work counters (statistics only), 32-bit to keep registers for the search; a
     // lane flushes them to the launch totals before they could wrap.
-    uint32_t scans = 0, probes = 0, tails = 0;
+    uint32_t scans = 0, probes = 0, tails = 0, shared = 0;
     unsigned int err = 0;
     const unsigned long long deadline = P.time_limit_ns ? P.ctrl->t_start + P.time_limit_ns : 0ull;
     bool have_source = true;  // seed tickets / frontier not yet exhausted
@@ -1221,13 +1290,14 @@ __global__ void __launch_bounds__(256, MINB) k_enumerate(EnumParams P) {
                 break;
             }
         }
-        const unsigned long long c = run_item<LASTLOOP, MODE>(S, P, scans, probes, tails, err, deadline);
+        const unsigned long long c = run_item<LASTLOOP, MODE>(S, P, scans, probes, tails, shared, err, deadline);
         if (lane == 0 && c) atomicAdd(P.counts + S.item_plan, c);
-        if ((scans | probes | tails) >= (1u << 30)) {
+        if ((scans | probes | tails | shared) >= (1u << 30)) {
             atomicAdd(&P.ctrl->scan_entries, (unsigned long long)scans);
             atomicAdd(&P.ctrl->probes, (unsigned long long)probes);
             atomicAdd(&P.ctrl->tail_lists, (unsigned long long)tails);
-            scans = probes = tails = 0;
+            if (lane == 0) atomicAdd(&P.ctrl->shared_last, (unsigned long long)shared);
+            scans = probes = tails = shared = 0;
         }
         __syncwarp();
     }
@@ -1240,6 +1310,7 @@ __global__ void __launch_bounds__(256, MINB) k_enumerate(EnumParams P) {
         if (scans64) atomicAdd(&P.ctrl->scan_entries, scans64);
         if (probes64) atomicAdd(&P.ctrl->probes, probes64);
         if (tails) atomicAdd(&P.ctrl->tail_lists, (unsigned long long)tails);
+        if (shared) atomicAdd(&P.ctrl->shared_last, (unsigned long long)shared);
         if (err) atomicOr(&P.ctrl->error, err);
     }
 }
@@ -1322,7 +1393,7 @@ __global__ void k_expand_bound(EnumParams P, const WorkItem *items, const unsign
         const WorkItem *it = items + i;
         const DevPlan *pl = P.plans + it->plan;
         const uint32_t d = it->depth;
-        if (d + 1 >= pl->tail_start) {
+        if (d >= pl->expand_stop) {
             if (lane == 0) acc += 1;  // passes through unchanged
             continue;
         }

@@ -532,6 +532,12 @@ std::vector<HostPlan> build_plans(const Query &q, uint16_t query_id, uint32_t nl
         }
         dp.tail = tail;
         dp.nterms = (uint32_t)terms.size();
+        if (hp.tail_start == (int)n && n >= 4) {
+            dp.shared_last = 1;
+            for (uint8_t b : hp.bn[n - 1])
+                if (b == n - 2) dp.shared_last = 0;
+        }
+        dp.expand_stop = (uint8_t)(dp.shared_last ? n - 2 : hp.tail_start - 1);
         plans.push_back(hp);
     }
     return plans;

@@ -123,7 +123,8 @@ typedef struct csm_stats {
     uint64_t graph_launches;        /* batches replayed from a CUDA graph */
     uint64_t replans;               /* re-plannings triggered by relation-size drift */
     uint64_t donations_refused;     /* donations not made because the donation ring was full */
-    uint64_t reserved[1];
+    uint64_t enum_shared_last;      /* last query levels counted once for all vertices matched at
+                                       the level above (the last vertex is not adjacent to it) */
 } csm_stats;
 
 /* Fills `cfg` with the defaults (algorithm 0 with all switches on, as main.cpp). */

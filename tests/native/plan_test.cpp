@@ -129,6 +129,13 @@ int main() {
                     if (all_back != (lv.nlf_bitmap == CSM_NO_BITMAP)) return fail("implied NLF filter", qn, (int)pi);
                 }
                 const int ts = hp.tail_start;
+                // The last level is shared by the candidates of level n - 2 exactly when it has
+                // no backward neighbour there (and no tail follows); expansion then stops at n - 2.
+                bool shared = ts == (int)n && n >= 4;
+                for (uint8_t b : hp.bn[n - 1])
+                    if (b == n - 2) shared = false;
+                if ((hp.dev.shared_last != 0) != shared) return fail("shared last level", qn, (int)pi);
+                if (hp.dev.expand_stop != (shared ? n - 2 : (uint32_t)ts - 1)) return fail("expansion stop", qn, (int)pi);
                 for (uint32_t d = (uint32_t)ts; d < n; d++) {
                     if (q.degree(hp.order[d]) != 1) return fail("tail vertex is not a leaf", qn, (int)pi);
                     if ((int)hp.bn[d][0] >= ts) return fail("tail parent inside the tail", qn, (int)pi);

@@ -14,7 +14,7 @@ from helpers import clique, cycle, path, random_graph, small_workload, star
 pytestmark = pytest.mark.gpu
 
 
-def check_stream(w, queries=None, batches=None, rows=False, **cfg):
+def check_stream(w, queries=None, batches=None, rows=False, stats=None, **cfg):
     queries = w.queries if queries is None else queries
     batches = w.batches if batches is None else batches
     if rows:
@@ -38,6 +38,8 @@ def check_stream(w, queries=None, batches=None, rows=False, **cfg):
                 assert np.array_equal(eng.embeddings(qi, -1), o.rows(-1)), f"batch {bi} query {qi} negative rows"
             totals[0] += r["pos"]
             totals[1] += r["neg"]
+    if stats is not None:
+        stats.append(eng.stats())
     eng.close()
     return totals
 
@@ -92,6 +94,38 @@ def test_multi_query_mixed_sizes():
 def test_heavy_vertex_dense8():
     w = small_workload("c3", scale=0.0005, batch=2000, nqueries=2)
     check_stream(w)
+
+
+def query_graph(labels, edges):
+    s, d = zip(*edges)
+    return QueryGraph(np.asarray(labels, dtype=np.uint32), np.array(s, dtype=np.uint32), np.array(d, dtype=np.uint32),
+                      np.zeros(len(edges), dtype=np.uint32))
+
+
+K23 = [(0, 2), (0, 3), (0, 4), (1, 2), (1, 3), (1, 4)]
+HOUSE = [(0, 1), (1, 2), (2, 3), (3, 0), (0, 4), (1, 4)]
+LADDER = [(0, 1), (1, 2), (3, 4), (4, 5), (0, 3), (1, 4), (2, 5)]
+
+
+@pytest.mark.parametrize("strategy", [0, 1, 2, 3])
+@pytest.mark.parametrize("order", [0, 1])
+def test_last_level_shared_by_the_level_above(strategy, order):
+    """Plans whose last query vertex is not adjacent to the vertex matched before it count the
+    last level once per prefix and subtract, per vertex above, whether that vertex is itself a
+    candidate (injectivity): same labels (the subtraction applies) and distinct labels (it
+    cannot), with deletions, under every search strategy."""
+    rng = np.random.default_rng(11)
+    n = 1500
+    vl, s, d, el = random_graph(n, 15000, 2, rng)
+    data, batches = gen.make_stream(n, s, d, el, rng, n_ins=1200, n_del=300, batch=500)
+    data = DataGraph(vl, data.src, data.dst, data.elabels)
+    queries = [query_graph([0] * 5, K23), query_graph([0, 0, 1, 1, 1], K23),
+               query_graph([0, 1, 0, 1, 1], HOUSE), query_graph([0] * 6, LADDER)]
+    w = gen.Workload("shared-last", data, batches, queries, 500)
+    st = []
+    tot = check_stream(w, stats=st, search_strategy=strategy, matching_order=order)
+    assert tot[0] > 0 and tot[1] > 0
+    assert st[0].enum_shared_last > 0
 
 
 def test_edge_cases_in_batches():
