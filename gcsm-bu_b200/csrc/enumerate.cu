@@ -56,6 +56,7 @@ struct __align__(16) WarpState {
     uint32_t t_size[CSM_TAIL_MAXKEYS];
     uint32_t t_flag[CSM_TAIL_MAXKEYS];
     uint32_t t_excl[CSM_TAIL_MAXKEYS];
+    uint32_t t_cur[CSM_TAIL_MAXKEYS];  // cursor of a probed list while an intersection is counted
     unsigned long long msize[CSM_TAIL_MAXMASKS];
     // Lane-parallel tail: per key whose parent is matched before the counting level, its
     // list and the list size left after the flag rule and the shared prefix.
@@ -281,13 +282,86 @@ __device__ void enter_level(WarpState &S, const EnumParams &P, const DevPlan *pl
     if (d + 1 == pl->tail_start && pl->tail_start < pl->n && pl->tail.lane_par) prep_tail_shared(S, P, pl, d);
 }
 
-// Number of injective assignments of the tail leaves for the full prefix f[0..E-1].
+// Size of the intersection of the tail lists in `mask` (at least two), each under its flag rule,
+// without the prefix vertices f[0..E-1]: the warp scans the smallest list 32 entries at a time.
+// A chunk's entries ascend, so every other list keeps a cursor: the 32 entries at the cursor
+// are read with one coalesced load and shuffles find each candidate; when the chunk reaches past
+// them, a 32-ary warp search brackets the window and lanes search inside it.
+__device__ uint32_t tail_intersection(WarpState &S, const EnumParams &P, const DevTail *T, uint32_t nkeys,
+                                      uint32_t mask, uint32_t E, uint32_t &probes) {
+    const uint32_t lane = lane_id();
+    uint32_t k0 = 0, best = 0xFFFFFFFFu;
+    for (uint32_t k = 0; k < nkeys; k++)
+        if (((mask >> k) & 1u) && S.t_size[k] < best) {
+            best = S.t_size[k];
+            k0 = k;
+        }
+    if (lane < nkeys) S.t_cur[lane] = 0;
+    __syncwarp();
+    const bool old0 = __ldg(&T->key_old[k0]) != 0;
+    uint32_t cnt = 0;
+    for (uint32_t base = 0; base < best; base += 32) {
+        const uint32_t idx = base + lane;
+        bool ok = idx < best;
+        uint32_t w = 0;
+        if (ok) {
+            const uint32_t e = __ldg(P.g.pool + S.t_off[k0] + idx);
+            w = e >> 1;
+            ok = !(old0 && (e & 1u));
+            if (w >= P.g.V) {
+                record_bad(P, CSM_BAD_ENTRY, e, S.t_off[k0] + idx, 700 + E);
+                ok = false;
+            }
+        }
+        for (uint32_t z = 0; ok && z < E; z++) ok = S.f[z] != w;
+        const uint32_t vmask = __ballot_sync(0xffffffffu, idx < best);
+        const uint32_t target = __shfl_sync(0xffffffffu, w, 31 - __clz(vmask));
+        const uint32_t key_hi = (target + 1) << 1;
+        for (uint32_t k = 0; k < nkeys; k++) {
+            if (k == k0 || !((mask >> k) & 1u)) continue;
+            if (!__any_sync(0xffffffffu, ok)) break;
+            const uint32_t *L = P.g.pool + S.t_off[k];
+            const uint32_t size = S.t_size[k], c0 = S.t_cur[k];
+            const uint32_t win = c0 + lane < size ? __ldg(L + c0 + lane) : 0xFFFFFFFFu;
+            const uint32_t below = __ballot_sync(0xffffffffu, win < key_hi);
+            uint32_t e = 0xFFFFFFFFu, hi;
+            if (below != 0xffffffffu) {
+                hi = c0 + __popc(below);
+                const uint32_t pos = shfl_lower_bound(win, w << 1);
+                const uint32_t got = __shfl_sync(0xffffffffu, win, pos);
+                if ((got >> 1) == w && got != 0xFFFFFFFFu) e = got;
+            } else {
+                hi = warp_lower_bound(L, c0 + 32, size, key_hi, lane);
+                if (ok) e = find_entry(L + c0, hi - c0, w);
+            }
+            if (ok) {
+                probes++;
+                ok = e != 0xFFFFFFFFu && !(__ldg(&T->key_old[k]) && (e & 1u));
+            }
+            __syncwarp();
+            if (lane == 0) S.t_cur[k] = hi;
+            __syncwarp();
+        }
+        cnt += __popc(__ballot_sync(0xffffffffu, ok));
+    }
+    return cnt;
+}
+
+// Number of injective assignments of the tail vertices for the full prefix f[0..E-1].
 __device__ unsigned long long tail_count(WarpState &S, const EnumParams &P, const DevPlan *pl,
                                          uint32_t &probes) {
     const uint32_t lane = lane_id();
     const DevTail *T = &pl->tail;
     const uint32_t nkeys = __ldg(&T->nkeys);
+    const uint32_t nmasks = __ldg(&T->nmasks);
     const uint32_t E = pl->tail_start;
+    // Lists whose size is used alone need their batch entries and the prefix vertices they
+    // hold; intersections check both entry by entry.
+    uint32_t single = 0;
+    for (uint32_t mi = 0; mi < nmasks; mi++) {
+        const uint32_t m = __ldg(&T->mask[mi]);
+        if (__popc(m) == 1) single |= m;
+    }
     if (lane < nkeys) {
         const uint32_t rel = __ldg(&T->key_rel[lane]);
         const uint32_t x = S.f[__ldg(&T->key_parent[lane])];
@@ -295,21 +369,23 @@ __device__ unsigned long long tail_count(WarpState &S, const EnumParams &P, cons
         S.t_off[lane] = ms.x;
         S.t_size[lane] = ms.y;
         // Flagged entries of this list = batch edges of (rel, x) in this phase.
-        S.t_flag[lane] = __ldg(&T->key_old[lane]) ? flagged_in_list(P, rel, x) : 0u;
+        S.t_flag[lane] = (__ldg(&T->key_old[lane]) && ((single >> lane) & 1u)) ? flagged_in_list(P, rel, x) : 0u;
         S.t_excl[lane] = 0;
     }
     __syncwarp();
-    // Prefix vertices that sit in a tail list are not available to the leaves.
+    // Prefix vertices that sit in a list sized alone are not available to its vertex.
+    uint32_t nprobe = 0;
     for (uint32_t pi = lane; pi < nkeys * E; pi += 32) {
         const uint32_t k = pi / E;
+        if (!((single >> k) & 1u)) continue;
         if (!((__ldg(&T->key_excl[k]) >> (pi % E)) & 1u)) continue;  // other labels are never in the list
         const uint32_t z = S.f[pi % E];
         const uint32_t e = find_entry(P.g.pool + S.t_off[k], S.t_size[k], z);
+        nprobe++;
         if (e != 0xFFFFFFFFu && !(__ldg(&T->key_old[k]) && (e & 1u))) atomicAdd(&S.t_excl[k], 1u);
     }
-    if (lane == 0) probes += nkeys * E;
+    probes += nprobe;
     __syncwarp();
-    const uint32_t nmasks = __ldg(&T->nmasks);
     for (uint32_t mi = 0; mi < nmasks; mi++) {
         const uint32_t mask = __ldg(&T->mask[mi]);
         unsigned long long size;
@@ -317,38 +393,7 @@ __device__ unsigned long long tail_count(WarpState &S, const EnumParams &P, cons
             const uint32_t k = __ffs(mask) - 1;
             size = (unsigned long long)S.t_size[k] - S.t_flag[k] - S.t_excl[k];
         } else {
-            // Intersection of several lists: scan the smallest, probe the others.
-            uint32_t k0 = 0, best = 0xFFFFFFFFu;
-            for (uint32_t k = 0; k < nkeys; k++)
-                if (((mask >> k) & 1u) && S.t_size[k] < best) {
-                    best = S.t_size[k];
-                    k0 = k;
-                }
-            const bool old0 = __ldg(&T->key_old[k0]) != 0;
-            uint32_t cnt = 0;
-            for (uint32_t base = 0; base < best; base += 32) {
-                const uint32_t idx = base + lane;
-                bool ok = idx < best;
-                uint32_t w = 0;
-                if (ok) {
-                    const uint32_t e = __ldg(P.g.pool + S.t_off[k0] + idx);
-                    w = e >> 1;
-                    ok = !(old0 && (e & 1u));
-                    if (w >= P.g.V) {
-                        record_bad(P, CSM_BAD_ENTRY, e, S.t_off[k0] + idx, 700 + E);
-                        ok = false;
-                    }
-                }
-                for (uint32_t z = 0; ok && z < E; z++) ok = S.f[z] != w;
-                for (uint32_t k = 0; ok && k < nkeys; k++) {
-                    if (k == k0 || !((mask >> k) & 1u)) continue;
-                    const uint32_t e = find_entry(P.g.pool + S.t_off[k], S.t_size[k], w);
-                    ok = e != 0xFFFFFFFFu && !(__ldg(&T->key_old[k]) && (e & 1u));
-                    probes++;
-                }
-                cnt += __popc(__ballot_sync(0xffffffffu, ok));
-            }
-            size = cnt;
+            size = tail_intersection(S, P, T, nkeys, mask, E, probes);
         }
         if (lane == 0) S.msize[mi] = size;
     }

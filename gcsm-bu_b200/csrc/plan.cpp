@@ -318,8 +318,11 @@ void for_each_partition(int m, const std::function<void(const std::vector<int> &
     partitions_from(1, 0, a, fn);
 }
 
-// Builds the tail bookkeeping for leaves at depths [tail_start, n).  Returns false when the
-// tail exceeds the device limits (the caller then shortens it).
+// Builds the tail bookkeeping for the vertices at depths [tail_start, n).  They are pairwise
+// non-adjacent and every neighbour of theirs is matched before tail_start, so each one's
+// candidates are the intersection of its backward-neighbour lists (its keys), and the number of
+// injective assignments is a polynomial in intersection sizes.  Returns false when the tail
+// exceeds the device limits (the caller then shortens it).
 bool build_tail(const Query &q, const HostPlan &hp, int qe, const RelOf &rel_of, DevTail &tail,
                 std::vector<DevTailTerm> &terms) {
     const int n = (int)hp.order.size();
@@ -327,20 +330,26 @@ bool build_tail(const Query &q, const HostPlan &hp, int qe, const RelOf &rel_of,
     terms.clear();
     if (hp.tail_start >= n) return true;
     struct Leaf {
-        int key;
+        uint16_t keys;  // bit k: key k is one of the vertex's lists
         uint32_t label;
     };
     std::vector<Leaf> leaves;
     std::vector<std::tuple<int, int, int>> keys;  // (parent depth, rel, old)
     for (int d = hp.tail_start; d < n; d++) {
-        int p = hp.bn[d][0];
-        uint32_t u = hp.order[d], pu = hp.order[p];
-        int rel = rel_of(pu, u);
-        int old = q.qe_index[pu * q.nv + u] > qe ? 1 : 0;
-        auto k = std::make_tuple(p, rel, old);
-        int ki = (int)(std::find(keys.begin(), keys.end(), k) - keys.begin());
-        if (ki == (int)keys.size()) keys.push_back(k);
-        leaves.push_back({ki, q.vlabel[u]});
+        const uint32_t u = hp.order[d];
+        Leaf leaf{0, q.vlabel[u]};
+        for (uint8_t p : hp.bn[d]) {
+            if ((int)p >= hp.tail_start) return false;  // not a tail: a neighbour in the tail
+            uint32_t pu = hp.order[p];
+            int rel = rel_of(pu, u);
+            int old = q.qe_index[pu * q.nv + u] > qe ? 1 : 0;
+            auto k = std::make_tuple((int)p, rel, old);
+            int ki = (int)(std::find(keys.begin(), keys.end(), k) - keys.begin());
+            if (ki == (int)keys.size()) keys.push_back(k);
+            if (ki >= CSM_TAIL_MAXKEYS) return false;
+            leaf.keys |= (uint16_t)(1u << ki);
+        }
+        leaves.push_back(leaf);
     }
     if (keys.size() > CSM_TAIL_MAXKEYS) return false;
     tail.nkeys = (uint8_t)keys.size();
@@ -351,14 +360,14 @@ bool build_tail(const Query &q, const HostPlan &hp, int qe, const RelOf &rel_of,
         // A key's relation fixes its leaves' label.
         uint32_t leaf_label = 0;
         for (auto &l : leaves)
-            if (l.key == (int)k) leaf_label = l.label;
+            if ((l.keys >> k) & 1u) leaf_label = l.label;
         uint16_t excl = 0;
         for (int d = 0; d < n; d++)
             if (q.vlabel[hp.order[d]] == leaf_label) excl |= (uint16_t)(1u << d);
         tail.key_excl[k] = excl;
     }
-    std::map<uint32_t, std::vector<int>> classes;  // label -> leaf key ids
-    for (auto &l : leaves) classes[l.label].push_back(l.key);
+    std::map<uint32_t, std::vector<uint16_t>> classes;  // label -> the key sets of its vertices
+    for (auto &l : leaves) classes[l.label].push_back(l.keys);
     if (classes.size() > CSM_TAIL_MAXCLASSES) return false;
     std::vector<uint16_t> masks;
     auto mask_id = [&](uint16_t m) -> int {
@@ -369,7 +378,7 @@ bool build_tail(const Query &q, const HostPlan &hp, int qe, const RelOf &rel_of,
     };
     int c = 0;
     for (auto &cl : classes) {
-        const std::vector<int> &ks = cl.second;
+        const std::vector<uint16_t> &ks = cl.second;
         const int m = (int)ks.size();
         if (m > 7) return false;
         tail.class_term_begin[c] = (uint16_t)terms.size();
@@ -383,7 +392,7 @@ bool build_tail(const Query &q, const HostPlan &hp, int qe, const RelOf &rel_of,
             std::vector<uint16_t> bm(nb, 0);
             std::vector<int> bs(nb, 0);
             for (int i = 0; i < m; i++) {
-                bm[a[i]] |= (uint16_t)(1u << ks[i]);
+                bm[a[i]] |= ks[i];  // a block's vertices share one candidate: all their lists
                 bs[a[i]]++;
             }
             int64_t coef = 1;
@@ -472,6 +481,9 @@ std::vector<HostPlan> build_plans(const Query &q, uint16_t query_id, uint32_t nl
         HostPlan hp;
         // Cartesian tail: query leaves after the starting edge move to the end of the order
         // (they constrain nothing else), and depth >= tail_start is counted arithmetically.
+        // The tail then grows backwards over every last head vertex adjacent to no tail vertex:
+        // its neighbours are all matched before it, so given the head it is independent of the
+        // other tail vertices too, and its candidates are an intersection of head lists.
         int tail_start = (int)n;
         if (opt.cartesian && !opt.materialize && n > 2) {
             std::vector<uint8_t> head(order.begin(), order.begin() + 2), leaves;
@@ -479,6 +491,17 @@ std::vector<HostPlan> build_plans(const Query &q, uint16_t query_id, uint32_t nl
             tail_start = (int)head.size();
             head.insert(head.end(), leaves.begin(), leaves.end());
             order = head;
+            const int leaf_start = tail_start;
+            while (tail_start > 2) {
+                bool free_vertex = true;
+                for (uint32_t t = (uint32_t)tail_start; t < n; t++)
+                    if (q.adjacent(order[tail_start - 1], order[t])) free_vertex = false;
+                if (!free_vertex) break;
+                tail_start--;
+            }
+            // Without leaves, one or two such vertices are counted faster by the last-level
+            // loops (the shared last level covers two).
+            if (leaf_start == (int)n && (int)n - tail_start < 3) tail_start = (int)n;
         }
         hp.order = order;
         hp.bn.assign(n, {});
@@ -559,7 +582,8 @@ std::string describe_plans(const Query &q, const std::vector<HostPlan> &plans) {
             os << ") ";
         }
         os << "\n    tail: " << (hp.tail_start < (int)hp.order.size() ? "from depth " + std::to_string(hp.tail_start) : std::string("none"))
-           << ", " << hp.terms.size() << " terms\n";
+           << ", " << hp.terms.size() << " terms" << (hp.dev.shared_last ? ", last level shared by the level above" : "")
+           << "\n";
     }
     return os.str();
 }

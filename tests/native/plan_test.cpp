@@ -2,9 +2,11 @@
 //  - every order is a permutation that starts with the updated query edge's endpoints;
 //  - the backward neighbours of each depth are exactly the query neighbours matched earlier,
 //    so every query edge is checked once;
-//  - tail vertices are leaves whose neighbour is matched before the tail;
+//  - every neighbour of a tail vertex is matched before the tail (leaves, and the vertices the
+//    tail grows over);
 //  - the tail's inclusion-exclusion polynomial, evaluated the way the enumeration kernel does,
-//    equals a brute-force count of injective leaf assignments on random candidate lists.
+//    equals a brute-force count of injective tail assignments on random candidate lists (a tail
+//    vertex's candidates: the intersection of its lists).
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -25,18 +27,29 @@ int fail(const char *what, int qn, int plan) {
     return 1;
 }
 
-// Brute force: number of maps leaf -> element of its list, injective within each label class.
-uint64_t brute(const std::vector<std::vector<int>> &lists, const std::vector<int> &leaf_key,
+bool in_list(const std::vector<int> &l, int x) {
+    for (int y : l)
+        if (y == x) return true;
+    return false;
+}
+
+// Brute force: number of maps tail vertex -> element of all its lists, injective within each
+// label class.
+uint64_t brute(const std::vector<std::vector<int>> &lists, int universe, const std::vector<uint16_t> &leaf_keys,
                const std::vector<uint32_t> &leaf_label, size_t i, std::vector<int> &chosen) {
-    if (i == leaf_key.size()) return 1;
+    if (i == leaf_keys.size()) return 1;
     uint64_t total = 0;
-    for (int x : lists[leaf_key[i]]) {
+    for (int x = 0; x < universe; x++) {
+        bool cand = true;
+        for (size_t k = 0; k < lists.size(); k++)
+            if (((leaf_keys[i] >> k) & 1u) && !in_list(lists[k], x)) cand = false;
+        if (!cand) continue;
         bool clash = false;
         for (size_t j = 0; j < i; j++)
             if (leaf_label[j] == leaf_label[i] && chosen[j] == x) clash = true;
         if (clash) continue;
         chosen[i] = x;
-        total += brute(lists, leaf_key, leaf_label, i + 1, chosen);
+        total += brute(lists, universe, leaf_keys, leaf_label, i + 1, chosen);
     }
     return total;
 }
@@ -137,28 +150,33 @@ int main() {
                 if ((hp.dev.shared_last != 0) != shared) return fail("shared last level", qn, (int)pi);
                 if (hp.dev.expand_stop != (shared ? n - 2 : (uint32_t)ts - 1)) return fail("expansion stop", qn, (int)pi);
                 for (uint32_t d = (uint32_t)ts; d < n; d++) {
-                    if (q.degree(hp.order[d]) != 1) return fail("tail vertex is not a leaf", qn, (int)pi);
-                    if ((int)hp.bn[d][0] >= ts) return fail("tail parent inside the tail", qn, (int)pi);
+                    if (hp.bn[d].size() != q.nbrs[hp.order[d]].size()) return fail("tail neighbour after the tail", qn, (int)pi);
+                    for (uint8_t b : hp.bn[d])
+                        if ((int)b >= ts) return fail("tail neighbour inside the tail", qn, (int)pi);
                 }
                 if (ts >= (int)n) continue;
                 // Evaluate the tail polynomial as the kernel does, on random candidate lists.
                 const DevTail &T = hp.dev.tail;
-                std::vector<int> leaf_key;
+                std::vector<uint16_t> leaf_keys;
                 std::vector<uint32_t> leaf_label;
                 for (uint32_t d = (uint32_t)ts; d < n; d++) {
-                    const int p = hp.bn[d][0];
-                    const uint32_t u = hp.order[d], pu = hp.order[p];
-                    const int rel = rel_of(pu, u);
-                    const int old = q.qe_index[pu * nv + u] > (int)pi ? 1 : 0;
-                    int key = -1;
-                    for (int k = 0; k < T.nkeys; k++)
-                        if (T.key_parent[k] == p && T.key_rel[k] == rel && T.key_old[k] == old) key = k;
-                    if (key < 0) return fail("leaf without a tail key", qn, (int)pi);
-                    for (uint32_t j = 0; j < n; j++) {
-                        const bool same = q.vlabel[hp.order[j]] == q.vlabel[u];
-                        if (same != (((T.key_excl[key] >> j) & 1u) != 0)) return fail("exclusion depths", qn, (int)pi);
+                    const uint32_t u = hp.order[d];
+                    uint16_t keys = 0;
+                    for (uint8_t p : hp.bn[d]) {
+                        const uint32_t pu = hp.order[p];
+                        const int rel = rel_of(pu, u);
+                        const int old = q.qe_index[pu * nv + u] > (int)pi ? 1 : 0;
+                        int key = -1;
+                        for (int k = 0; k < T.nkeys; k++)
+                            if (T.key_parent[k] == p && T.key_rel[k] == rel && T.key_old[k] == old) key = k;
+                        if (key < 0) return fail("tail vertex without a tail key", qn, (int)pi);
+                        for (uint32_t j = 0; j < n; j++) {
+                            const bool same = q.vlabel[hp.order[j]] == q.vlabel[u];
+                            if (same != (((T.key_excl[key] >> j) & 1u) != 0)) return fail("exclusion depths", qn, (int)pi);
+                        }
+                        keys |= (uint16_t)(1u << key);
                     }
-                    leaf_key.push_back(key);
+                    leaf_keys.push_back(keys);
                     leaf_label.push_back(q.vlabel[u]);
                 }
                 for (int trial = 0; trial < 20; trial++) {
@@ -192,8 +210,8 @@ int main() {
                         }
                         total *= (unsigned long long)s;
                     }
-                    std::vector<int> chosen(leaf_key.size());
-                    const uint64_t want = brute(lists, leaf_key, leaf_label, 0, chosen);
+                    std::vector<int> chosen(leaf_keys.size());
+                    const uint64_t want = brute(lists, universe, leaf_keys, leaf_label, 0, chosen);
                     if (total != want) {
                         std::printf("tail count %llu, brute force %llu\n", total, (unsigned long long)want);
                         return fail("tail polynomial", qn, (int)pi);
