@@ -104,10 +104,20 @@ struct DevPlan {
     // them (injectivity; possible only when the two query vertices share a label).
     uint8_t shared_last;
     // Items of this depth or deeper pass a breadth-first expansion unexpanded: tail_start - 1,
-    // or n - 2 for shared_last plans (whose level n - 2 stays whole inside one item).
+    // n - 2 for shared_last plans (whose level n - 2 stays whole inside one item), tail_start - 2
+    // for pendant plans (whose counting level is never entered).
     uint8_t expand_stop;
-    uint8_t pad2[2];
+    // Pendant counting level: the counting level c = tail_start - 1 has one backward neighbour,
+    // at depth memo_depth, every tail list hangs off c itself, and no prefix vertex shares a label
+    // with c or a tail vertex.  The count below a prefix is then a function of the one data vertex
+    // at memo_depth, precomputed for every vertex per phase into table memo_slot (CSM_NO_MEMO:
+    // not pendant; CSM_MEMO_PENDING: pendant, no table assigned yet).
+    uint8_t memo_slot;
+    uint8_t memo_depth;
 };
+
+#define CSM_NO_MEMO 0xFFu
+#define CSM_MEMO_PENDING 0xFEu
 
 // Work item of the persistent enumeration: a partial embedding with `depth` fixed vertices
 // and the range [lo, hi) of candidates still to scan at level `depth` (for depth 0 the range

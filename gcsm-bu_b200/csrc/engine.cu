@@ -173,7 +173,7 @@ Engine::~Engine() {
                    g_.vlab, d_plans_, d_terms_, d_upd_src_, d_upd_dst_, d_upd_lab_, d_upd_del_, d_keys_raw_, d_keys_,
                    d_sort_temp_, bs_.eff, bs_.heads, bs_.nheads, bs_.seg_nins, bs_.seg_ndel, bs_.seg_end, bs_.scr_y,
                    bs_.scr_lb, bs_.counters, bs_.error, d_ctrl_, d_queue_, d_seq_, d_seed_lo_, d_ticket_prefix_,
-                   d_counts_, d_frontier_[0], d_frontier_[1], d_rows_, d_misc_, d_rel_delta_, d_touched_};
+                   d_counts_, d_frontier_[0], d_frontier_[1], d_rows_, d_misc_, d_rel_delta_, d_touched_, d_memo_};
     for (void *p : dev)
         if (p) cudaFree(p);
     if (h_pin_) cudaFreeHost(h_pin_);
@@ -510,6 +510,50 @@ csm_status Engine::install_plans(const std::vector<EdgeStats> &stats) {
     }
     begin.push_back((uint32_t)plans.size());
     if (!plans_.empty() && plans.size() != plans_.size()) return fail(CSM_ERR_STATE, "re-planning changed the plan count");
+    // Pendant plans with the same counting level and tail read one table: its entries do not
+    // depend on the depths or on the query.  At most kMaxPendantTables tables (V entries each);
+    // further pendant plans, or all of them when the tables do not fit, count normally.
+    constexpr size_t kMaxPendantTables = 16;
+    std::vector<std::vector<int64_t>> sigs;
+    std::vector<uint32_t> memo_plan;
+    for (uint32_t i = 0; i < plans.size(); i++) {
+        DevPlan &dp = plans[i].dev;
+        if (dp.memo_slot != CSM_MEMO_PENDING) continue;
+        const DevLevel &lv = dp.lv[dp.tail_start - 1];
+        const DevTail &t = dp.tail;
+        std::vector<int64_t> sig{lv.bn_rel[0], lv.old_mask & 1, lv.nlf_bitmap, t.nkeys, t.nmasks, t.nclasses};
+        for (int k = 0; k < t.nkeys; k++) sig.insert(sig.end(), {t.key_rel[k], t.key_old[k]});
+        for (int k = 0; k < t.nmasks; k++) sig.push_back(t.mask[k]);
+        for (int c = 0; c <= t.nclasses; c++) sig.push_back(t.class_term_begin[c]);
+        for (const DevTailTerm &term : plans[i].terms) {
+            sig.insert(sig.end(), {term.coef, term.nf});
+            for (int j = 0; j < term.nf; j++) sig.push_back(term.f[j]);
+        }
+        size_t slot = std::find(sigs.begin(), sigs.end(), sig) - sigs.begin();
+        if (slot == sigs.size()) {
+            if (sigs.size() == kMaxPendantTables) continue;
+            sigs.push_back(sig);
+            memo_plan.push_back(i);
+        }
+        dp.memo_slot = (uint8_t)slot;
+    }
+    if (memo_plan.size() > memo_cap_) {
+        if (d_memo_) cudaFree(d_memo_);
+        d_memo_ = nullptr;
+        memo_cap_ = 0;
+        if (dev_alloc(&d_memo_, memo_plan.size() * (size_t)g_.V) == cudaSuccess) {
+            memo_cap_ = memo_plan.size();
+        } else {
+            (void)cudaGetLastError();
+            d_memo_ = nullptr;
+        }
+    }
+    if (memo_plan.size() > memo_cap_) {
+        for (auto &hp : plans)
+            if (hp.dev.memo_slot != CSM_NO_MEMO) hp.dev.memo_slot = CSM_MEMO_PENDING;
+        memo_plan.clear();
+    }
+    memo_plan_ = std::move(memo_plan);
     std::vector<DevPlan> dplans;
     std::vector<DevTailTerm> terms;
     for (auto &hp : plans) {
@@ -1229,6 +1273,13 @@ csm_status Engine::enumerate_phase(uint32_t phase, uint32_t m, cudaStream_t s) {
         D.frontier = frontier;
         launch_ctrl_reset(sc_.ctrl, 0, nfront, s);
         stats_.kernel_launches++;
+    }
+    if (!rows && !memo_plan_.empty()) {
+        // Tables of the pendant plans for this phase's graph and flags.
+        for (size_t t = 0; t < memo_plan_.size(); t++)
+            launch_pendant_counts(D, memo_plan_[t], d_memo_ + t * (size_t)g_.V, s);
+        stats_.kernel_launches += memo_plan_.size();
+        D.memo = d_memo_;
     }
     launch_enumerate(D, blocks_, warps_per_block_, occupancy_, s);
     stats_.enum_launches++;

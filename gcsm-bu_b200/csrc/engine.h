@@ -204,6 +204,12 @@ class Engine {
     uint64_t time_limit_us_ = 0;              // per enumeration launch; 0 = none
     csm_status deferred_ = CSM_OK;            // timeout / overflow of this batch, reported at its end
     bool last_loop_ = false;                  // launch the kernel variant with the last-level loop
+    // Pendant plans (DevPlan.memo_slot): table t is filled each phase by the kernel of plan
+    // memo_plan_[t] and read by every plan with the same counting level and tail; d_memo_ holds
+    // memo_cap_ tables of V entries.
+    unsigned long long *d_memo_ = nullptr;
+    size_t memo_cap_ = 0;
+    std::vector<uint32_t> memo_plan_;
     unsigned long long last_frontier_rows_ = 0;
     // CUDA graphs of whole batches (depth-first strategies), keyed by what the capture bakes in.
     struct GraphKey {

@@ -185,7 +185,8 @@ __device__ void prep_tail_shared(WarpState &S, const EnumParams &P, const DevPla
 // Lane-parallel tail, per lane: the tail count of the prefix f[0..d-1] + v, where v is this
 // lane's candidate at depth d (for d == 1 the prefix is the seed edge (x0, v)).  Only for
 // plans whose masks are single keys (no list intersections).
-__device__ unsigned long long tail_count_lane(const WarpState &S, const EnumParams &P, const DevPlan *pl,
+__device__ unsigned long long tail_count_lane(const uint32_t *ts_base, const uint32_t *f, const EnumParams &P,
+                                              const DevPlan *pl,
                                               uint32_t d, uint32_t x0, uint32_t v, uint32_t shared_hit,
                                               uint32_t &probes) {
     const DevTail *T = &pl->tail;
@@ -201,7 +202,7 @@ __device__ unsigned long long tail_count_lane(const WarpState &S, const EnumPara
         if (pd < d && d >= 2) {
             // Shared list: only this lane's candidate may still sit in it (looked up by the
             // warp beforehand, bit k of shared_hit).
-            left = S.ts_base[k] - ((shared_hit >> k) & 1u);
+            left = ts_base[k] - ((shared_hit >> k) & 1u);
             (void)old;
         } else {
             const uint32_t x = (pd == d) ? v : x0;  // d >= 2: pd == d; d == 1: parent 0 or 1
@@ -210,7 +211,7 @@ __device__ unsigned long long tail_count_lane(const WarpState &S, const EnumPara
             const uint32_t excl = __ldg(&T->key_excl[k]);
             for (uint32_t j = 0; j <= d; j++) {
                 if (j == pd || !((excl >> j) & 1u)) continue;
-                const uint32_t z = (j == d) ? v : (d == 1 ? x0 : S.f[j]);
+                const uint32_t z = (j == d) ? v : (d == 1 ? x0 : f[j]);
                 const uint32_t e = find_entry(P.g.pool + ms.x, ms.y, z);
                 probes++;
                 if (e != 0xFFFFFFFFu && !(old && (e & 1u))) left--;
@@ -498,6 +499,9 @@ __device__ bool try_donate(WarpState &S, const EnumParams &P, const DevPlan *pl,
     // A shared last level is counted once per prefix at depth n - 3: the two deepest levels of
     // a prefix stay with the warp that holds it (so neither is counted twice).
     const uint32_t top = pl->shared_last ? pl->n - 3u : d;
+    // Above a pendant counting level, buffered candidates are settled from the table, never
+    // entered: they are not handed out as items of the counting level either.
+    const uint32_t sib_end = pl->memo_slot != CSM_NO_MEMO ? E - 1u : E;
     for (uint32_t l = L0; l <= d && l <= top; l++) {
         const uint32_t lo = S.lo[l], hi = S.hi[l];
         const uint32_t minr = (l == 1) ? 64u : P.steal_min;
@@ -516,7 +520,7 @@ __device__ bool try_donate(WarpState &S, const EnumParams &P, const DevPlan *pl,
             return true;
         }
         const uint32_t nb = S.nbuf[l], ps = S.pos[l];
-        if (l < d && l + 1 < E && nb > ps) {
+        if (l < d && l + 1 < sib_end && nb > ps) {
             const uint32_t cnt = nb - ps;
             const uint32_t slot = reserve_slots(P, cnt);
             if (slot == 0xFFFFFFFFu) return false;
@@ -924,6 +928,28 @@ __device__ unsigned long long count_shared_last(WarpState &S, const EnumParams &
     return total;
 }
 
+// Pendant counting level c = d + 1 (DevPlan.memo_slot): every buffered candidate of level d
+// contributes the table entry of the data vertex at memo_depth (the candidate itself when that
+// depth is d).  Consumes the buffer.
+__device__ unsigned long long settle_pendant(WarpState &S, const EnumParams &P, const DevPlan *pl, uint32_t d,
+                                             uint32_t &tails) {
+    const uint32_t lane = lane_id();
+    const uint32_t ps = S.pos[d], k = S.nbuf[d] - ps;
+    const uint32_t md = pl->memo_depth;
+    const unsigned long long *table = P.memo + (size_t)pl->memo_slot * P.g.V;
+    unsigned long long v = 0;
+    if (lane < k) {
+        const uint32_t x = md == d ? S.buf[d][ps + lane] : S.f[md];
+        v = __ldg(table + x);
+        tails++;
+    }
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    __syncwarp();
+    if (lane == 0) S.pos[d] = S.nbuf[d];
+    __syncwarp();
+    return v;
+}
+
 // Runs one work item to completion (or until the device clock passes `deadline`, when that is
 // nonzero: the rest of the item is then dropped and CSM_ERRBIT_TIMEOUT set).  Returns the number
 // of matches counted.
@@ -999,6 +1025,11 @@ __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, uint32
             if (granted && !try_donate(S, P, pl, L0, d) && lane == 0) atomicAdd(&P.ctrl->hungry, 1u);
         }
         if (S.pos[d] < S.nbuf[d]) {
+            if (MODE == CSM_ENUM_MODE_COUNT && d + 2 == E && P.memo != nullptr && pl->memo_slot < CSM_MEMO_PENDING) {
+                // Pendant counting level below: each buffered candidate's count is a table entry.
+                cnt += settle_pendant(S, P, pl, d, tails);
+                continue;
+            }
             if (MODE == CSM_ENUM_MODE_COUNT && d + 2 == n && pl->shared_last) {
                 // The last level does not depend on these candidates: count it once for the
                 // prefix (first time here), then settle every buffered candidate at once.
@@ -1220,9 +1251,9 @@ __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, uint32
             if (ok) {
                 if (d == 1) {
                     const unsigned long long key = __ldg(P.keys + cand);
-                    t = tail_count_lane(S, P, pl, 1, P.kl.src(key), P.kl.dst(key), 0, probes);
+                    t = tail_count_lane(S.ts_base, S.f, P, pl, 1, P.kl.src(key), P.kl.dst(key), 0, probes);
                 } else {
-                    t = tail_count_lane(S, P, pl, d, 0, cand, shared_hit, probes);
+                    t = tail_count_lane(S.ts_base, S.f, P, pl, d, 0, cand, shared_hit, probes);
                 }
             }
             for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
@@ -1429,6 +1460,57 @@ __global__ void k_ctrl_reset(EnumControl *ctrl, uint32_t active, unsigned long l
 }
 
 // Upper bound of the next BFS level: sum over items of their smallest candidate list.
+// Table of a pendant plan (DevPlan.memo_slot): for every data vertex v, the count of its
+// counting level c for a prefix whose vertex at memo_depth is v — the candidates w of v's list
+// under the flag rule and c's NLF filter, each with its Cartesian tail, exactly as the
+// lane-parallel counting level sums them (no prefix exclusion can apply).  One warp per vertex.
+__global__ void k_pendant_counts(EnumParams P, uint32_t plan, unsigned long long *out) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const DevPlan *pl = P.plans + plan;
+    const uint32_t c = pl->tail_start - 1u;
+    const DevLevel *lv = &pl->lv[c];
+    const uint32_t rel = __ldg(&lv->bn_rel[0]);
+    const bool old = (__ldg(&lv->old_mask) & 1u) != 0;
+    const uint32_t nlf_id = __ldg(&lv->nlf_bitmap);
+    const uint32_t *nlf = nlf_id == CSM_NO_BITMAP ? nullptr : bitmap(P, nlf_id);
+    uint32_t scans = 0, probes = 0, tails = 0;
+    const uint32_t nw = gridDim.x * (blockDim.x >> 5);
+    for (uint32_t v = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); v < P.g.V; v += nw) {
+        const uint2 ms = list_of(P, rel, v, 900 + c);
+        unsigned long long acc = 0;
+        for (uint32_t base = 0; base < ms.y; base += 32) {
+            const uint32_t idx = base + lane;
+            if (idx >= ms.y) continue;
+            const uint32_t e = __ldg(P.g.pool + ms.x + idx);
+            const uint32_t w = e >> 1;
+            scans++;
+            bool ok = !(old && (e & 1u));
+            if (w >= P.g.V) {
+                record_bad(P, CSM_BAD_ENTRY, e, ms.x + idx, 900 + c);
+                ok = false;
+            }
+            if (ok && nlf) ok = test_bit(nlf, w);
+            if (ok) {
+                acc += tail_count_lane(nullptr, nullptr, P, pl, c, 0, w, 0, probes);
+                tails++;
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) out[v] = acc;
+    }
+    unsigned long long s64 = scans, p64 = probes, t64 = tails;
+    for (int o = 16; o > 0; o >>= 1) {
+        s64 += __shfl_xor_sync(0xffffffffu, s64, o);
+        p64 += __shfl_xor_sync(0xffffffffu, p64, o);
+        t64 += __shfl_xor_sync(0xffffffffu, t64, o);
+    }
+    if (lane == 0) {
+        if (s64) atomicAdd(&P.ctrl->scan_entries, s64);
+        if (p64) atomicAdd(&P.ctrl->probes, p64);
+        if (t64) atomicAdd(&P.ctrl->tail_lists, t64);
+    }
+}
+
 __global__ void k_expand_bound(EnumParams P, const WorkItem *items, const unsigned long long *nitems) {
     const uint32_t lane = threadIdx.x & 31u;
     const unsigned long long nw = (unsigned long long)gridDim.x * (blockDim.x >> 5);
@@ -1507,6 +1589,10 @@ void launch_seed_tickets(const DevPlan *plans, uint32_t nplans, const unsigned l
 
 void launch_ctrl_reset(EnumControl *ctrl, uint32_t active, unsigned long long nticket, cudaStream_t s) {
     k_ctrl_reset<<<1, 1, 0, s>>>(ctrl, active, nticket);
+}
+
+void launch_pendant_counts(const EnumParams &p, uint32_t plan, unsigned long long *out, cudaStream_t s) {
+    k_pendant_counts<<<148 * 8, 256, 0, s>>>(p, plan, out);
 }
 
 void launch_expand_bound(const EnumParams &p, const WorkItem *items, const unsigned long long *nitems,

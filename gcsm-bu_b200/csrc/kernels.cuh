@@ -113,6 +113,9 @@ struct EnumParams {
     // register-resident last-level loop is launched (the other variant leaves that code out,
     // which keeps the registers of the tail-counting paths).
     uint32_t last_loop;
+    // Pendant counting levels (DevPlan.memo_slot): per table, the count below a prefix for every
+    // data vertex at the plan's memo_depth; nullptr counts those levels like any other.
+    const unsigned long long *memo;
 };
 
 #define CSM_ROW_WORDS (1 + CSM_MAXQV)
@@ -129,6 +132,8 @@ void launch_seed_tickets(const DevPlan *plans, uint32_t nplans, const unsigned l
                          KeyLayout kl, uint32_t *seed_lo, uint32_t *ticket_prefix, EnumControl *ctrl,
                          cudaStream_t s);
 void launch_ctrl_reset(EnumControl *ctrl, uint32_t active, unsigned long long nticket, cudaStream_t s);
+// Fills table `out` (one entry per data vertex) for the pendant plan `plan` in this phase.
+void launch_pendant_counts(const EnumParams &p, uint32_t plan, unsigned long long *out, cudaStream_t s);
 void launch_expand_bound(const EnumParams &p, const WorkItem *items, const unsigned long long *nitems,
                          cudaStream_t s);
 

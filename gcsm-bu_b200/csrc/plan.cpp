@@ -561,6 +561,18 @@ std::vector<HostPlan> build_plans(const Query &q, uint16_t query_id, uint32_t nl
                 if (b == n - 2) dp.shared_last = 0;
         }
         dp.expand_stop = (uint8_t)(dp.shared_last ? n - 2 : hp.tail_start - 1);
+        dp.memo_slot = CSM_NO_MEMO;
+        const int c = hp.tail_start - 1;
+        if (hp.tail_start < (int)n && tail.lane_par && c >= 3 && hp.bn[c].size() == 1 && dp.lv[c].excl_mask == 0) {
+            bool pendant = true;
+            for (int k = 0; k < tail.nkeys; k++)
+                if (tail.key_parent[k] != c || (tail.key_excl[k] & ((1u << c) - 1u)) != 0) pendant = false;
+            if (pendant) {
+                dp.memo_slot = CSM_MEMO_PENDING;
+                dp.memo_depth = hp.bn[c][0];
+                dp.expand_stop = (uint8_t)(c - 1);
+            }
+        }
         plans.push_back(hp);
     }
     return plans;
@@ -583,6 +595,7 @@ std::string describe_plans(const Query &q, const std::vector<HostPlan> &plans) {
         }
         os << "\n    tail: " << (hp.tail_start < (int)hp.order.size() ? "from depth " + std::to_string(hp.tail_start) : std::string("none"))
            << ", " << hp.terms.size() << " terms" << (hp.dev.shared_last ? ", last level shared by the level above" : "")
+           << (hp.dev.memo_slot != CSM_NO_MEMO ? ", pendant counting level" : "")
            << "\n";
     }
     return os.str();

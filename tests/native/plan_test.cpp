@@ -148,7 +148,20 @@ int main() {
                 for (uint8_t b : hp.bn[n - 1])
                     if (b == n - 2) shared = false;
                 if ((hp.dev.shared_last != 0) != shared) return fail("shared last level", qn, (int)pi);
-                if (hp.dev.expand_stop != (shared ? n - 2 : (uint32_t)ts - 1)) return fail("expansion stop", qn, (int)pi);
+                // Pendant counting level c = ts - 1: one backward neighbour, every tail vertex
+                // hangs off c alone, single-list tail terms, and no vertex before c shares a label
+                // with c or with a tail vertex.
+                const int c = ts - 1;
+                bool pendant = ts < (int)n && c >= 3 && hp.bn[c].size() == 1 && hp.dev.tail.lane_par;
+                for (uint32_t d = (uint32_t)ts; pendant && d < n; d++)
+                    if (hp.bn[d].size() != 1 || hp.bn[d][0] != c) pendant = false;
+                for (int j = 0; pendant && j < c; j++)
+                    for (uint32_t d = (uint32_t)c; d < n; d++)
+                        if (q.vlabel[hp.order[j]] == q.vlabel[hp.order[d]]) pendant = false;
+                if ((hp.dev.memo_slot == CSM_MEMO_PENDING) != pendant) return fail("pendant counting level", qn, (int)pi);
+                if (pendant && hp.dev.memo_depth != hp.bn[c][0]) return fail("pendant table depth", qn, (int)pi);
+                if (hp.dev.expand_stop != (shared ? n - 2 : pendant ? (uint32_t)c - 1 : (uint32_t)ts - 1))
+                    return fail("expansion stop", qn, (int)pi);
                 for (uint32_t d = (uint32_t)ts; d < n; d++) {
                     if (hp.bn[d].size() != q.nbrs[hp.order[d]].size()) return fail("tail neighbour after the tail", qn, (int)pi);
                     for (uint8_t b : hp.bn[d])

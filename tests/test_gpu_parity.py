@@ -128,6 +128,29 @@ def test_last_level_shared_by_the_level_above(strategy, order):
     assert st[0].enum_shared_last > 0
 
 
+PENDANT = [(2, 3), (2, 4), (2, 5), (3, 4), (3, 5), (4, 5), (1, 2), (0, 1)]
+
+
+@pytest.mark.parametrize("strategy", [0, 1, 2, 3])
+def test_pendant_counting_level(strategy):
+    """A 4-clique with a two-vertex path hanging off it, the path's label absent from the clique:
+    plans that start inside the clique count the path from per-vertex tables filled each phase
+    (the table kernel, the settling of sibling buffers, and the donation and expansion limits)."""
+    rng = np.random.default_rng(5)
+    n = 1200
+    vl, s, d, el = random_graph(n, 16000, 3, rng)
+    data, batches = gen.make_stream(n, s, d, el, rng, n_ins=1200, n_del=300, batch=500)
+    data = DataGraph(vl, data.src, data.dst, data.elabels)
+    queries = [query_graph([0, 0, 1, 2, 1, 2], PENDANT), query_graph([2, 0, 1, 1, 1, 1], PENDANT)]
+    w = gen.Workload("pendant", data, batches, queries, 500)
+    with csm.Engine(search_strategy=strategy) as eng:
+        eng.load_query(queries[0])
+        eng.load_graph(data)
+        assert eng.describe(0).count("pendant counting level") > 0
+    tot = check_stream(w, search_strategy=strategy)
+    assert tot[0] > 0 and tot[1] > 0
+
+
 def test_edge_cases_in_batches():
     rng = np.random.default_rng(7)
     vl, s, d, el = random_graph(60, 300, 2, rng)
