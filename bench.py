@@ -487,11 +487,11 @@ def run_ours(args, w, world, rank, local):
                      "avg_launch_ms": 1e3 * enum_s / launches,
                      "traffic": (traffic["dram_bytes_per_algorithmic_byte"] * alg_bytes / launches) if traffic else None,
                      "l2_traffic": (traffic["lts_bytes_per_algorithmic_byte"] * alg_bytes / launches) if traffic else None,
-                     "traffic_note": "DRAM and L2 bytes per algorithmic byte measured by ncu over every enumeration "
-                                     "launch of one bench-shaped batch (c3, query 0, 1M updates; "
-                                     "profiles/enumerate_traffic.json), times this run's algorithmic bytes per "
-                                     "launch; the lists stay on chip, so the HBM fraction measures issue and "
-                                     "latency efficiency, not bandwidth" if traffic else None},
+                     "traffic_note": ("DRAM and L2 bytes per algorithmic byte measured by ncu over every enumeration "
+                                      "launch of one batch (" + traffic["workload"] + "; "
+                                      "profiles/enumerate_traffic.json), times this run's algorithmic bytes per "
+                                      "launch; the lists stay on chip, so the HBM fraction measures issue and "
+                                      "latency efficiency, not bandwidth") if traffic else None},
         "phase_ms_per_step": {"enumerate": 1e3 * enum_s / args.steps, "apply": 1e3 * apply_s / args.steps},
         "clocks": clk.summary(),
     }
