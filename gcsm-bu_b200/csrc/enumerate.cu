@@ -1048,8 +1048,9 @@ __device__ unsigned long long run_item(WarpState &S, const EnumParams &P, uint32
                 __syncwarp();
                 continue;
             }
-            // Siblings whose subtree is only the last level: count them together.
-            if (d + 2 == n && E == n && d >= 2 && MODE == CSM_ENUM_MODE_COUNT &&
+            // Siblings whose subtree is only the last level: count them together.  Tried once per
+            // buffer: when the lists are too long for it, they stay so for the later siblings.
+            if (d + 2 == n && E == n && d >= 2 && MODE == CSM_ENUM_MODE_COUNT && S.pos[d] == 0 &&
                 count_last_packed(S, P, pl, d, cnt, scans, probes))
                 continue;
             // Descend into the next buffered candidate.
