@@ -70,7 +70,7 @@ typedef struct csm_config {
     uint64_t materialize_rows;      /* >0: keep up to this many embedding rows per batch */
     int32_t blocks_per_sm;          /* persistent enumeration launch shape; 0 = automatic */
     int32_t warps_per_block;        /* 0 = automatic */
-    int32_t steal_chunk;            /* minimum candidate range split by work donation; 0 = auto */
+    int32_t steal_chunk;            /* minimum candidate range split by work donation; 0 = 8 */
     int32_t occupancy;              /* enumeration kernel built for 4, 5 or 6 resident 256-thread
                                        blocks per SM (fewer registers per thread); 0 = 4 */
     int32_t autotune_batches;       /* >0: over the first batches, time the enumeration under every
