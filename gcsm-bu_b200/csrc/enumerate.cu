@@ -941,8 +941,8 @@ __device__ unsigned long long settle_pendant(WarpState &S, const EnumParams &P, 
     if (lane < k) {
         const uint32_t x = md == d ? S.buf[d][ps + lane] : S.f[md];
         v = __ldg(table + x);
-        tails++;
     }
+    tails += k;  // warp-uniform, like every other use of the tail counter
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     __syncwarp();
     if (lane == 0) S.pos[d] = S.nbuf[d];
@@ -1372,7 +1372,8 @@ __global__ void __launch_bounds__(256, MINB) k_enumerate(EnumParams P) {
         if ((scans | probes | tails | shared) >= (1u << 30)) {
             atomicAdd(&P.ctrl->scan_entries, (unsigned long long)scans);
             atomicAdd(&P.ctrl->probes, (unsigned long long)probes);
-            atomicAdd(&P.ctrl->tail_lists, (unsigned long long)tails);
+            // The tail and shared-level counters are warp-uniform: one lane adds them.
+            if (lane == 0) atomicAdd(&P.ctrl->tail_lists, (unsigned long long)tails);
             if (lane == 0) atomicAdd(&P.ctrl->shared_last, (unsigned long long)shared);
             scans = probes = tails = shared = 0;
         }
