@@ -543,7 +543,12 @@ csm_status Engine::install_plans(const std::vector<EdgeStats> &stats) {
         if (d_memo_) cudaFree(d_memo_);
         d_memo_ = nullptr;
         memo_cap_ = 0;
-        if (dev_alloc(&d_memo_, memo_plan.size() * (size_t)g_.V) == cudaSuccess) {
+        // The tables are an optimisation: they only take memory the adjacency pool is unlikely
+        // to need (at most a quarter of what is free now).
+        size_t free_b = 0, total_b = 0;
+        const size_t want = memo_plan.size() * (size_t)g_.V * sizeof(unsigned long long);
+        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && want <= free_b / 4 &&
+            dev_alloc(&d_memo_, memo_plan.size() * (size_t)g_.V) == cudaSuccess) {
             memo_cap_ = memo_plan.size();
         } else {
             (void)cudaGetLastError();
